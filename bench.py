@@ -1,0 +1,343 @@
+"""Benchmark of the KG method-of-lines hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl kg|reference]
+
+Workload (one "step" = one PIRK2 time step, the stepper of the reference's
+evolve loop, main/evolve.f90:25): the single large FP64 solve of the
+benchmark description -- Nr = 2048 radial cells on r in [1.8, 400], 128 x 256
+theta x phi cells (reference grid integers Nx = 2048, Ny = 129, Nz = 257, two
+ghosts), Kerr-Schild M = 1, field mass 0.3, outflow outer boundary, CFL 0.25
+with the reference dt rule; seeded Gaussian shell (r0 ~ U[8,15], sigma 1.5)
+times sum_{l<=4} c_lm Y_lm, c_lm complex N(0, 1e-4).  Synthetic, seeded data;
+the state (5.7 GB per copy) is far larger than L2, so no flush is needed.
+The Berger-Oliger refinement levels of that description are not part of this
+measurement.
+
+Metric: grid-point-stage updates per second (GPSU/s) = interior points x RK
+stages x steps / time.  `value` is device time of K steps with the state
+resident in HBM (CUDA events on the solver's stream, max over ranks);
+`e2e` goes through the C ABI from pinned host memory: upload of the initial
+state, K x (kg_pirk2 + kg_diagnostic with its 8-byte mass read-back), download
+of the final state.
+
+With --gpus N (torchrun), every rank runs an independent replica on its own
+GPU (the path has no exchange step), `value` sums all ranks, scaling "weak".
+
+--impl reference times the CPU restatement of the reference's own path (the
+oracle, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(Nx=2048, Ny=129, Nz=257, xmin=1.8, xmax=400.0, m=0.3, CFL=0.25, seed=20240601)
+METRIC = "RK point-updates/s (FP64 PIRK2, Nr=2048 x Ntheta=128 x Nphi=256)"
+UNIT = "GPSU/s"
+# algorithmic bytes per stored point of each PIRK2 kernel (complex128 = 16 B per variable)
+#   stage_pirk_s1_psi: read u (5 vars) + write u_stage(1:4)               = 80 + 64
+#   stage_pirk_s1_pi : read u_stage(1:4), stale u_stage(5), u(5); write u_stage(5) = 64 + 16 + 16 + 16
+#   stage_pirk2_s2   : read u_stage, u_p(=u); write u                     = 80 + 80 + 80
+ALG_BYTES = {"stage_pirk_s1_psi": 144, "stage_pirk_s1_pi": 112, "stage_pirk2_s2": 240}
+PIRK2_MIN_BYTES = 416  # fused minimum per point-step: read u, stale Pi, u_stage, u; write u_stage, u
+
+
+def workload_config(w):
+    return {
+        "workload": "FP64 PIRK2 large solve: Nx=2048 Ny=129 Nz=257 (Nr=2048, Ntheta=128, Nphi=256), "
+                    "r in [1.8,400], Kerr-Schild M=1, m=0.3, outflow, CFL 0.25 reference dt rule",
+        "grid": [w["Nx"], w["Ny"], w["Nz"]],
+        "stepper": "pirk2",
+        "refinement": "none (single level)",
+        "l2": "inputs larger than L2 (5.7 GB per state copy)",
+        "seed": w["seed"],
+    }
+
+
+def interior_points(w):
+    return w["Nx"] * (w["Ny"] - 1) * (w["Nz"] - 1)
+
+
+def stored_points(w):
+    return (w["Nx"] + 5) * (w["Ny"] + 5) * (w["Nz"] + 1)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel):
+    """dram bytes per launch from the committed ncu summary, if there is one."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_c1.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(gpu_id), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(w, threads, nx_sample=64, steps=2):
+    """The oracle (CPU restatement of the reference path) on a radial slab of the
+    workload: same theta x phi grid, Nx = nx_sample cells, `steps` PIRK2 steps."""
+    from oracle.oracle import Oracle, set_threads
+    from kg_b200.initial_data import shell_ylm
+    set_threads(threads)
+    Nx = nx_sample
+    xmax = w["xmin"] + (w["xmax"] - w["xmin"]) * Nx / w["Nx"]
+    o = Oracle(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, CFL=w["CFL"], m=w["m"])
+    u0, _ = shell_ylm(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, seed=w["seed"], r0=8.0)
+    o.set_state(u0)
+    o.pirk2(1)  # warm
+    t0 = time.perf_counter()
+    o.pirk2(steps)
+    dt = time.perf_counter() - t0
+    gpsu = Nx * (w["Ny"] - 1) * (w["Nz"] - 1) * 2 * steps / dt
+    return gpsu, dt, f"PIRK2 x{steps} on the Nx={Nx} radial slab of the workload grid ({Nx}x{w['Ny']}x{w['Nz']})"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = WORKLOAD
+    threads = os.cpu_count() or 1
+    from oracle.oracle import Oracle, set_threads
+    from kg_b200.initial_data import shell_ylm
+    set_threads(threads)
+    Nx = 64
+    xmax = w["xmin"] + (w["xmax"] - w["xmin"]) * Nx / w["Nx"]
+    o = Oracle(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, CFL=w["CFL"], m=w["m"])
+    u0, _ = shell_ylm(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, seed=w["seed"], r0=8.0)
+    o.set_state(u0)
+    for _ in range(args.warmup):
+        o.pirk2(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.pirk2(1)
+    el = time.perf_counter() - t0
+    pts = Nx * (w["Ny"] - 1) * (w["Nz"] - 1)
+    val = pts * 2 * args.steps / el
+    sample = f"PIRK2 on the Nx={Nx} radial slab of the workload grid ({Nx}x{w['Ny']}x{w['Nz']}), one step per step"
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic (seeded)", "config": workload_config(w),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="kg", choices=["kg", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    from kg_b200 import ScalarField
+    from kg_b200.initial_data import shell_ylm_device
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    w = WORKLOAD
+    mol = ScalarField(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], m=w["m"], device=local,
+                      save=10 * 0.25 * 0.0018, l_max=8)
+    lib, h = mol._lib, mol.handle
+    u0, _ = shell_ylm_device(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], seed=w["seed"] + rank,
+                             device=f"cuda:{local}")
+    mol._ck(lib.kg_set_state_device(h, 0, C.c_void_p(u0.data_ptr())))
+    mol.synchronize()
+    stream = torch.cuda.ExternalStream(lib.kg_get_stream(h), device=f"cuda:{local}")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident timing
+    for _ in range(args.warmup):
+        mol.pirk2(1)
+    mol.synchronize()
+    nk = lib.kg_profile_kinds()
+    ms = (C.c_double * nk)()
+    cnt = (C.c_longlong * nk)()
+    lib.kg_profile_read(h, ms, cnt)
+    lib.kg_profile_enable(h, 1)
+    barrier()
+    torch.cuda.synchronize()
+    gpu_id = torch.cuda.get_device_properties(local).uuid
+    clocks = ClockSampler(f"GPU-{gpu_id}" if gpu_id else local)
+    launches0 = lib.kg_launch_count(h)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        mol.pirk2(1)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    launches = lib.kg_launch_count(h) - launches0
+    el_ms = e0.elapsed_time(e1)
+    lib.kg_profile_read(h, ms, cnt)
+    lib.kg_profile_enable(h, 0)
+    t = torch.tensor([el_ms], device=f"cuda:{local}", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    el_ms = float(t.item())
+    kinds = {lib.kg_profile_kind_name(i).decode(): (ms[i], cnt[i]) for i in range(nk) if cnt[i] > 0}
+
+    # other steppers, briefly (device-resident, same grid)
+    per_stepper = {}
+    stages = {"pirk2": 2, "pirk3": 3, "rk3": 3, "rk4": 4}
+    for meth in ("pirk3", "rk3", "rk4"):
+        getattr(mol, meth)(nsteps=1) if meth.startswith("rk") else getattr(mol, meth)(1)
+        mol.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n = 5
+        a0.record(stream)
+        getattr(mol, meth)(nsteps=n) if meth.startswith("rk") else getattr(mol, meth)(n)
+        a1.record(stream)
+        a1.synchronize()
+        per_stepper[meth] = interior_points(w) * stages[meth] * n / (a0.elapsed_time(a1) / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    state_bytes = 5 * 16 * stored_points(w)
+    host_u0 = torch.empty(u0.numel() * 2, dtype=torch.float64, pin_memory=True)
+    host_u0.copy_(torch.view_as_real(u0).reshape(-1))
+    host_out = torch.empty_like(host_u0)
+    del u0
+    mass = C.c_double(0.0)
+    Dp = C.POINTER(C.c_double)
+    p_in = C.cast(C.c_void_p(host_u0.data_ptr()), Dp)
+    p_out = C.cast(C.c_void_p(host_out.data_ptr()), Dp)
+    mol.density()
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    mol._ck(lib.kg_set_state(h, 0, p_in))
+    for l in range(1, args.steps + 1):
+        mol._ck(lib.kg_pirk2(h, 1))
+        mol._ck(lib.kg_diagnostic(h, l, C.byref(mass)))
+    mol._ck(lib.kg_get_state(h, 0, p_out))
+    f1.record(stream)
+    f1.synchronize()
+    t = torch.tensor([f0.elapsed_time(f1)], device=f"cuda:{local}", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+
+    pts = interior_points(w)
+    value = world * pts * 2 * args.steps / (el_ms / 1e3)
+    e2e_value = world * pts * 2 * args.steps / (e2e_ms / 1e3)
+
+    # roofline of the dominant kernel
+    dom = max(kinds.items(), key=lambda kv: kv[1][0])[0] if kinds else "stage_pirk2_s2"
+    dms, dcnt = kinds.get(dom, (0.0, 1))
+    peak, peak_kind = measured_peaks()
+    alg = ALG_BYTES.get(dom, 0) * stored_points(w)
+    achieved = alg / (dms / dcnt / 1e3) / 1e9 if dcnt else 0.0
+    tr = profile_traffic(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": tr,
+                "algorithmic_bytes_per_launch": alg, "avg_launch_ms": dms / dcnt if dcnt else None}
+    step_bytes = PIRK2_MIN_BYTES * stored_points(w)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded Gaussian shell x Y_lm, l<=4)",
+            "config": dict(workload_config(w), parallelism=f"replicas x{world}"),
+            "roofline": roofline,
+            "step_bandwidth_gbs": step_bytes / (el_ms / args.steps / 1e3) / 1e9,
+            "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in kinds.items()},
+            "steppers_gpsu": dict(per_stepper, pirk2=value / world),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
+                    "d2h_bytes_per_step": (state_bytes + 8 * args.steps) / args.steps},
+            "gpu_launches": int(launches), "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, secs, sample = cpu_baseline(w, threads)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                                "seconds": secs}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    mol.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,172 @@
+/*
+ * kg_capi.h -- C ABI of the B200 method-of-lines solver for the Klein-Gordon
+ * field on a Kerr-Schild / Schwarzschild background in (r, theta, phi).
+ *
+ * Every entry point is a plain C function over plain pointers and sizes.  Each
+ * replaces one type-bound procedure of the reference's Fortran objects
+ * (FlavioRosales/KG), cited beside it, so a Fortran host binds it through
+ * iso_c_binding and keeps its evolve loop unchanged.  The MPI slab
+ * decomposition of the reference is replaced by whole-grid residency on one
+ * GPU: the solver owns every state array in device memory, the ghost-zone,
+ * pole-parity and outer-boundary fills run on the device, and send_recv_xL/xR
+ * have no counterpart.
+ *
+ * Conventions
+ *   - Grid integers follow the reference namelist: Nx radial cells, Ny theta
+ *     points (theta has Ny-1 cells plus pole ghosts), Nz phi points (period
+ *     Nz-1, one duplicated point), g_pts ghosts (must be 2).
+ *   - Host state arrays use the reference layout u(1:5, -g:Nx+g, -g:Ny+g, 0:Nz)
+ *     of complex(8): a flat array of 2*5*(Nx+2g+1)*(Ny+2g+1)*(Nz+1) doubles,
+ *     (re, im) pairs, variable index fastest.
+ *   - Every function returns KG_OK (0) or a positive KG_E* code; the text of
+ *     the last error of a handle is kg_last_error(h).  Nothing aborts the host.
+ *   - A handle is used by one host thread at a time; all its device work is
+ *     ordered on one CUDA stream (kg_get_stream).
+ */
+#ifndef KG_CAPI_H
+#define KG_CAPI_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum kg_status {
+  KG_OK = 0,
+  KG_EINVAL = 1,     /* bad argument or parameter combination */
+  KG_ENOMEM = 2,     /* device or host allocation failed */
+  KG_ECUDA = 3,      /* a CUDA call failed (message in kg_last_error) */
+  KG_ESTATE = 4,     /* call not valid in the handle's current state */
+  KG_ETIMEOUT = 5,   /* a bounded device wait ran out */
+  KG_ENODEV = 6      /* no usable sm_100 device */
+};
+
+enum kg_metric { KG_KERR_SCHILD = 0, KG_SCHW_EF = 1 };
+enum kg_bc_rmax { KG_OUTFLOW = 0, KG_INFLOW = 1 };
+
+/* Mirrors the reference namelist &input (main/global_numbers.f90:76-90) and
+ * the arguments of scalar_field_constructor (MoL/diagnostic_lib.f90:40-42). */
+typedef struct kg_params {
+  int Nx, Ny, Nz, g_pts;
+  double xmin, xmax, tmin, tmax, CFL;
+  double a, M_bh, m;          /* spin, black-hole mass, field mass */
+  int metric;                 /* enum kg_metric */
+  int bc_rmax;                /* enum kg_bc_rmax */
+  int n_det;                  /* detectors, >= 2 */
+  int l_max;                  /* Y_lm order of the detector projection */
+  double dt_override;         /* > 0 replaces the reference dt rule */
+  double save_;               /* diagnostic cadence in time units (namelist save_) */
+} kg_params;
+
+typedef struct kg_solver kg_solver;
+
+/* --- lifetime ---------------------------------------------------------- */
+
+/* scalar_field_constructor (MoL/diagnostic_lib.f90:40-151) together with
+ * mesh_refinement_boundary/create (MoL/mesh_refinement_lib.f90:100-147),
+ * geometry_load_metric/inverse (MoL/geometry.f90:92-352) and the dt rule
+ * (MoL/diagnostic_lib.f90:101-107).  Allocates all device state, builds the
+ * metric tables and detector list, zeroes the state.  device < 0: current. */
+int kg_create(const kg_params *p, int device, kg_solver **out);
+/* no reference counterpart (the reference never deallocates) */
+int kg_destroy(kg_solver *h);
+const char *kg_last_error(const kg_solver *h);
+/* scalars: dx, dy, dz, dt, t, xmin, xmax, Nt, r_max (9 doubles) */
+int kg_get_scalars(const kg_solver *h, double *out9);
+int kg_set_time(kg_solver *h, double t);
+int kg_set_dt(kg_solver *h, double dt);
+/* the CUDA stream (cudaStream_t) the handle orders its work on */
+void *kg_get_stream(const kg_solver *h);
+/* bytes of device memory held by the handle */
+size_t kg_device_bytes(const kg_solver *h);
+/* wait until the handle's queued device work has finished (the steppers and
+ * diagnostics enqueue and return; the reference's calls were synchronous) */
+int kg_synchronize(kg_solver *h);
+
+/* --- state exchange (the Fortran host's MoL%u, MoL%u_stage, ...) -------- */
+
+/* which: 0 = u, 1 = u_stage, 2 = u_stage_2, 3 = u_p.  Host arrays in the
+ * Fortran layout above; the device keeps r-fastest planes per variable. */
+int kg_set_state(kg_solver *h, int which, const double *host_u);
+int kg_get_state(kg_solver *h, int which, double *host_u);
+/* same, from / to a device buffer in the Fortran layout */
+int kg_set_state_device(kg_solver *h, int which, const double *dev_u);
+int kg_get_state_device(kg_solver *h, int which, double *dev_u);
+
+/* --- time steppers (MoL/lines_method_lib.f90) ---------------------------- */
+
+/* pirk2 (:271-332), nsteps consecutive calls */
+int kg_pirk2(kg_solver *h, int nsteps);
+/* pirk3 (:334-408) */
+int kg_pirk3(kg_solver *h, int nsteps);
+/* rk3 (:211-269) with rhs(1) = the type-bound rhs_* set applied to u */
+int kg_rk3(kg_solver *h, int nsteps);
+/* rk4 (:411-474) with the same rhs */
+int kg_rk4(kg_solver *h, int nsteps);
+
+/* --- RHS and boundaries (parity hooks) ----------------------------------- */
+
+/* rhs_phi/psi1/psi2/psi3/pi (:671-753) evaluated on host vars (Fortran layout);
+ * bit v of var_mask selects rhs variable v; unselected outputs are left as
+ * passed in rhs_inout. */
+int kg_rhs(kg_solver *h, const double *host_vars, double *host_rhs_inout, unsigned var_mask);
+/* boundary_xL, xR, yL, yR, zL, zR (:507-597) on u, bits 0..5 in that order,
+ * applied in that order; xR 'inflow' copies from u_p. */
+int kg_boundary(kg_solver *h, unsigned face_mask);
+/* send_recv_xL / send_recv_xR (:475-505): single domain, nothing to exchange */
+int kg_send_recv(kg_solver *h);
+
+/* --- geometry ------------------------------------------------------------- */
+
+/* 2-D (r, theta) tables, each (Ny+2g+1) x (Nx+2g+1) doubles, r fastest, in the
+ * order alpha, beta^r, d_r beta^r, sqrt(gamma), gamma^rr, gamma^rphi,
+ * gamma^thth, gamma^phph (MoL/geometry.f90:273-352; phi-independent). */
+int kg_get_metric(kg_solver *h, double *host_tables8);
+/* replace the tables above (a host that built its own geometry) */
+int kg_set_metric(kg_solver *h, const double *host_tables8);
+/* validate_inverse_metric (MoL/geometry.f90:409-492): error counts of the
+ * 4-metric and 3-metric identities at tolerance 1e-10 over the whole grid */
+int kg_validate_inverse_metric(kg_solver *h, int *errors_4d, int *errors_3d);
+
+/* --- diagnostics (MoL/diagnostic_lib.f90) --------------------------------- */
+
+/* density (:277-289): rho from the current u, kept on the device */
+int kg_density(kg_solver *h);
+/* download rho ((Nz+1) x (Ny+2g+1) x (Nx+2g+1) doubles, r fastest) */
+int kg_get_density(kg_solver *h, double *host_rho);
+/* Mass_scalar = integrate(rho*sqrtg) (:214, tools/integral.f90:646-674) */
+int kg_mass_scalar(kg_solver *h, double *out);
+/* currents_ADM + currents_detectors (:219-229, :252-274): momentum(3, n_det),
+ * component fastest; detectors outside the grid are left as passed */
+int kg_currents_detectors(kg_solver *h, double *host_momentum);
+/* proyector_detectors (:231-250): alm(l, m, d) complex, l fastest then m
+ * (-l_max..l_max) then detector; detectors outside the grid are left as passed */
+int kg_proyector_detectors(kg_solver *h, double *host_alm);
+/* diagnostic(index) (:185-217): density is not recomputed (as in the
+ * reference); every `save` steps currents and a_lm are refreshed on device. */
+int kg_diagnostic(kg_solver *h, int index, double *mass_out);
+/* detector radii and vertex indices (1-based) */
+int kg_get_detectors(kg_solver *h, double *r_det, int *index_det);
+/* sph_harmonics (tools/FFT_sph.f90:282-336) on the vertex grid:
+ * Ylm(l, m, j, k) complex, l fastest, m = -L..L, theta then phi */
+int kg_sph_harmonics(kg_solver *h, int L, double *host_ylm);
+
+/* --- instrumentation (no reference counterpart; the reference times its
+ * evolve loop with MPI_Wtime, main/evolve.f90:7, main/save_gnuplot.f90:158) */
+
+/* when on, every kernel launch of the handle is bracketed by CUDA events on
+ * the handle's stream and its duration is accumulated per kernel kind */
+int kg_profile_enable(kg_solver *h, int on);
+/* accumulated milliseconds and launch counts per kernel kind (arrays of
+ * kg_profile_kinds() entries); clears the accumulators */
+int kg_profile_read(kg_solver *h, double *ms, long long *launches);
+int kg_profile_kinds(void);
+const char *kg_profile_kind_name(int kind);
+/* total kernel launches issued by the handle since creation */
+long long kg_launch_count(const kg_solver *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KG_CAPI_H */

@@ -1,0 +1,1147 @@
+// kg_capi.cu -- the C ABI (include/kg_capi.h): solver handle, device memory,
+// geometry set-up, the time-stepper drivers and the diagnostics front end.
+//
+// Host code here does only set-up that the reference also does once at
+// start-up (grid, metric tables, detector and Y_lm tables; MoL/geometry.f90,
+// MoL/diagnostic_lib.f90:40-151, tools/FFT_sph.f90:282-336) and the
+// orchestration of device launches.  Every time step, RHS evaluation, boundary
+// fill, reduction and projection runs in the kernels of kg_stencil.cu,
+// kg_boundary.cu and kg_diag.cu.  There is no host fallback: without a usable
+// device kg_create fails with KG_ENODEV.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/kg_capi.h"
+#include "kg_device.cuh"
+#include "kg_internal.h"
+#include "kg_diag.h"
+
+using kg::Grid;
+using kg::Metric;
+
+namespace {
+
+enum { T_ALPHA = 0, T_BETA, T_DXBETA, T_SQRTG, T_ASG, T_GRR, T_GRP, T_GPP, T_ASG_GTT, T_ASG_GRR, T_A_GPP, T_AM2,
+       T_GTT, T_COUNT };
+
+}  // namespace
+
+struct kg_solver {
+  kg_params p;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  Grid g;
+  int Nx, Ny, Nz, NI, NJ, NK, PI;
+  double dx, dy, dz, dt, t, xmin, xmax, r_max;
+  int Nt = 0, save = 1;
+  int L = 10;
+  size_t bytes = 0;
+  // host geometry (2-D, index i + NI*j)
+  std::vector<double> x1d, y1d, tables;  // tables: T_COUNT x NJ x NI (unpadded)
+  std::vector<double> gdn, gup, gam;     // 16, 16, 9 tables of NI*NJ
+  // device memory
+  double* dmet = nullptr;                // T_COUNT x NJ x PI
+  double2* U = nullptr;                  // u (5 variables)
+  double2* S = nullptr;                  // u_stage (6 slots; slot 4/5 alternate for Pi)
+  double2* T = nullptr;                  // u_stage_2 (6 slots)
+  double2* RK = nullptr;                 // RK stage buffers R1, R2 and accumulator (15 slots)
+  double2* UP = nullptr;                 // u_p for the boundary hook
+  double2* HV = nullptr;                 // rhs hook input / output (10 slots)
+  double2* stage_buf = nullptr;          // Fortran-layout staging buffer
+  size_t stage_bytes = 0;
+  int stage_planes = 0;
+  double* rho = nullptr;
+  double* partials = nullptr;            // mass partial sums + result
+  int s_cur = 4, t_cur = 4;              // slot holding the current Pi stage value
+  // detectors and projection
+  int n_det = 5;
+  std::vector<double> r_det;
+  std::vector<int> index_det;
+  int* d_int = nullptr;                  // active[n_det], i_r[n_det], i_th[Ny], th_flag[Ny], i_ph[Nz]
+  double* d_dbl = nullptr;               // w_r, w_th, w_ph, sint, normP, cosm, sinm
+  double2* shells = nullptr;             // n_det x 4 x Ny x Nz
+  double2* alm = nullptr;                // (L+1) x (2L+1) x n_det
+  double* flux = nullptr;                // 3 x n_det
+  kg::ShellInterp si;
+  const double *normP = nullptr, *cosm = nullptr, *sinm = nullptr, *sint = nullptr;
+  std::vector<int> active;
+  // instrumentation
+  long long launches = 0;
+  int prof_on = 0;
+  struct Rec { int kind; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+};
+
+#define KG_CK(call)                                                                   \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
+      return KG_ECUDA;                                                                \
+    }                                                                                 \
+  } while (0)
+
+namespace {
+
+int set_err(kg_solver* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int dalloc(kg_solver* h, void** p, size_t n) {
+  cudaError_t e = cudaMalloc(p, n);
+  if (e != cudaSuccess) {
+    h->err = std::string("cudaMalloc(") + std::to_string(n) + "): " + cudaGetErrorString(e);
+    *p = nullptr;
+    return KG_ENOMEM;
+  }
+  h->bytes += n;
+  cudaMemsetAsync(*p, 0, n, h->stream);
+  return KG_OK;
+}
+
+size_t field_bytes(const kg_solver* h) { return (size_t)h->g.fs * sizeof(double2); }
+
+double2* fld(double2* base, const Grid& g, int v) { return base + (long long)v * g.fs; }
+
+// kernel kinds reported by kg_profile_read: the 13 stage kinds, then these
+enum { PK_GHOST = 13, PK_FACE, PK_RHS, PK_CONVERT, PK_DENSITY, PK_MASS, PK_SHELL, PK_FLUX, PK_PROJECT, PK_COUNT };
+const char* const kPkNames[PK_COUNT] = {
+    "stage_pirk_s1_psi", "stage_pirk_s1_pi", "stage_pirk2_s2", "stage_pirk3_s2_psi", "stage_pirk3_s2_pi",
+    "stage_pirk3_s3", "stage_rk3_1", "stage_rk3_2", "stage_rk3_3", "stage_rk4_1", "stage_rk4_2", "stage_rk4_3",
+    "stage_rk4_4", "ghost_fill", "boundary_face", "rhs", "layout_convert", "density", "mass_reduce",
+    "shell_interp", "flux_reduce", "ylm_project"};
+
+cudaEvent_t take_event(kg_solver* h) {
+  if (!h->pool.empty()) {
+    cudaEvent_t e = h->pool.back();
+    h->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct Prof {
+  kg_solver* h;
+  int kind, n;
+  cudaEvent_t a = nullptr;
+  Prof(kg_solver* h_, int kind_, int n_) : h(h_), kind(kind_), n(n_) {
+    if (h->prof_on) {
+      a = take_event(h);
+      cudaEventRecord(a, h->stream);
+    }
+  }
+  ~Prof() {
+    h->launches += n;
+    if (a) {
+      cudaEvent_t b = take_event(h);
+      cudaEventRecord(b, h->stream);
+      h->recs.push_back({kind, a, b});
+    }
+  }
+};
+
+// ---- geometry (MoL/mesh_refinement_lib.f90:100-147, MoL/geometry.f90:92-406) ----
+void build_geometry(kg_solver* h) {
+  const int NI = h->NI, NJ = h->NJ, g = h->p.g_pts;
+  const double pi = std::acos(-1.0);
+  const double dxr = (h->p.xmax - h->p.xmin) / 1.0;
+  h->xmin = h->p.xmin + 0.0 * dxr;
+  h->xmax = h->p.xmin + 1.0 * dxr;
+  h->dx = (h->xmax - h->xmin) / (double)h->Nx;
+  h->dy = pi / (double)(h->Ny - 1);
+  h->dz = 2.0 * pi / (double)(h->Nz - 1);
+  h->x1d.resize(NI);
+  h->y1d.resize(NJ);
+  for (int i = -g; i <= h->Nx + g; ++i) h->x1d[i + g] = h->xmin + (double)(i + g) * h->dx;
+  for (int j = -g; j <= h->Ny + g; ++j) h->y1d[j + g] = -h->dy / 2.0 + (double)j * h->dy;
+  h->r_max = h->x1d[NI - 1];
+  const double dxx = h->x1d[1] - h->x1d[0];
+  double c1 = dxx, c2 = std::exp(h->p.xmin) * h->dy, c3 = std::exp(h->p.xmin) * std::sin(h->dy / 2.0) * h->dz;
+  double mn = c1 < c2 ? c1 : c2;
+  mn = mn < c3 ? mn : c3;
+  h->dt = h->p.CFL * mn;
+  if (h->p.dt_override > 0.0) h->dt = h->p.dt_override;
+  h->Nt = (int)((h->p.tmax - h->p.tmin) / h->dt);
+  if (h->Nt % 2 != 0) h->Nt += 1;
+  h->t = h->p.tmin;
+  h->save = (int)(h->p.tmin + std::ceil((h->p.save_ > 0 ? h->p.save_ : h->dt) / h->dt));
+  if (h->save < 1) h->save = 1;
+
+  const size_t n2 = (size_t)NI * NJ;
+  h->gdn.assign(16 * n2, 0.0);
+  h->gup.assign(16 * n2, 0.0);
+  h->gam.assign(9 * n2, 0.0);
+  auto GD = [&](int a, int b, size_t q) -> double& { return h->gdn[(a * 4 + b) * n2 + q]; };
+  auto GU = [&](int a, int b, size_t q) -> double& { return h->gup[(a * 4 + b) * n2 + q]; };
+  const double M = h->p.M_bh, A = h->p.a;
+  for (int jj = 0; jj < NJ; ++jj)
+    for (int ii = 0; ii < NI; ++ii) {
+      const size_t q = ii + (size_t)NI * jj;
+      const double x = h->x1d[ii], y = h->y1d[jj];
+      if (h->p.metric == KG_KERR_SCHILD) {
+        const double cy = std::cos(y), sy = std::sin(y);
+        const double c2v = cy * cy, s2 = sy * sy;
+        const double rho2 = x * x + (A * A) * c2v;
+        GD(0, 0, q) = -1.0 + 2.0 * M * x / rho2;
+        GD(0, 1, q) = (2.0 * M * x / rho2);
+        GD(0, 2, q) = 0.0;
+        GD(0, 3, q) = -(2.0 * A * M * x * s2 / rho2);
+        GD(1, 0, q) = GD(0, 1, q);
+        GD(1, 1, q) = (1.0 + 2.0 * M * x / rho2);
+        GD(1, 2, q) = 0.0;
+        GD(1, 3, q) = (-(A * (1.0 + 2.0 * M * x / rho2) * s2));
+        GD(2, 2, q) = (x * x + (A * A) * c2v);
+        GD(3, 0, q) = GD(0, 3, q);
+        GD(3, 1, q) = GD(1, 3, q);
+        const double ax = (A * A + x * x);
+        GD(3, 3, q) = ((ax * ax) - (A * A) * (-(2.0 * M * x) + A * A + x * x) * s2) * s2 / rho2;
+      } else {
+        const double sy = std::sin(y);
+        GD(0, 0, q) = -(1.0 - 2.0 * M / x);
+        GD(0, 1, q) = 2.0 * M / x;
+        GD(1, 0, q) = GD(0, 1, q);
+        GD(1, 1, q) = 1.0 + 2.0 * M / x;
+        GD(2, 2, q) = x * x;
+        GD(3, 3, q) = x * x * (sy * sy);
+      }
+    }
+  // boundary_theta_dn: last theta row <- the row before (metric is phi-independent)
+  for (int ii = 0; ii < NI; ++ii) {
+    const size_t qt = ii + (size_t)NI * (NJ - 1), qs = ii + (size_t)NI * (NJ - 2);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) GD(a, b, qt) = GD(a, b, qs);
+    GD(0, 2, qt) = -GD(0, 2, qs);
+    GD(1, 2, qt) = -GD(1, 2, qs);
+  }
+  std::vector<double> sqrtg(n2), alpha(n2), beta(3 * n2), dxbeta(n2);
+  for (size_t q = 0; q < n2; ++q) {
+    GD(1, 0, q) = GD(0, 1, q); GD(2, 0, q) = GD(0, 2, q); GD(3, 0, q) = GD(0, 3, q);
+    GD(2, 1, q) = GD(1, 2, q); GD(3, 1, q) = GD(1, 3, q); GD(3, 2, q) = GD(2, 3, q);
+    sqrtg[q] = std::sqrt(GD(2, 2, q) * (GD(1, 1, q) * GD(3, 3, q) - GD(1, 3, q) * GD(1, 3, q)));
+  }
+  for (size_t q = 0; q < n2; ++q) {
+    const double g00 = GD(0, 0, q), g01 = GD(0, 1, q), g03 = GD(0, 3, q), g11 = GD(1, 1, q), g13 = GD(1, 3, q),
+                 g22 = GD(2, 2, q), g33 = GD(3, 3, q);
+    const double det =
+        ((g33 * g11 - g13 * g13) * g00 - g33 * (g01 * g01) + 2.0 * g13 * g03 * g01 - g11 * (g03 * g03)) * g22;
+    const double idetg = 1.0 / det;
+    GU(0, 0, q) = g22 * (g11 * g33 - g13 * g13) * idetg;
+    GU(0, 1, q) = g22 * (g13 * g03 - g01 * g33) * idetg;
+    GU(0, 2, q) = 0.0;
+    GU(0, 3, q) = g22 * (g13 * g01 - g11 * g03) * idetg;
+    GU(1, 1, q) = g22 * (g33 * g00 - g03 * g03) * idetg;
+    GU(1, 2, q) = 0.0;
+    GU(1, 3, q) = g22 * (-(g13 * g00) + g03 * g01) * idetg;
+    GU(2, 2, q) =
+        ((g33 * g11 - g13 * g13) * g00 - g33 * (g01 * g01) + 2.0 * g13 * g03 * g01 - g11 * (g03 * g03)) * idetg;
+    GU(2, 3, q) = 0.0;
+    GU(3, 3, q) = g22 * (g11 * g00 - g01 * g01) * idetg;
+  }
+  for (int ii = 0; ii < NI; ++ii) {  // boundary_theta_up
+    const size_t qt = ii + (size_t)NI * (NJ - 1), qs = ii + (size_t)NI * (NJ - 2);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) GU(a, b, qt) = GU(a, b, qs);
+    GU(0, 2, qt) = -GU(0, 2, qs);
+    GU(1, 2, qt) = -GU(1, 2, qs);
+  }
+  for (size_t q = 0; q < n2; ++q) {
+    GU(1, 0, q) = GU(0, 1, q); GU(2, 0, q) = GU(0, 2, q); GU(3, 0, q) = GU(0, 3, q);
+    GU(2, 1, q) = GU(1, 2, q); GU(3, 1, q) = GU(1, 3, q); GU(3, 2, q) = GU(2, 3, q);
+    const double al = std::sqrt(-1.0 / GU(0, 0, q));
+    alpha[q] = al;
+    const double a2 = al * al;
+    beta[q] = a2 * GU(0, 1, q);
+    beta[n2 + q] = a2 * GU(0, 2, q);
+    beta[2 * n2 + q] = a2 * GU(0, 3, q);
+  }
+  for (size_t q = 0; q < n2; ++q) {
+    const double a2 = alpha[q] * alpha[q];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        h->gam[(a * 3 + b) * n2 + q] = GU(a + 1, b + 1, q) + beta[a * n2 + q] * beta[b * n2 + q] / a2;
+  }
+  {  // dx_beta = real(dx1(dcmplx(beta(1)))), MoL/geometry.f90:344
+    const double res = 0.50 / h->dx;
+    for (int jj = 0; jj < NJ; ++jj) {
+      const double* F = beta.data() + (size_t)NI * jj;
+      double* D = dxbeta.data() + (size_t)NI * jj;
+      const int n = NI - 1;
+      D[0] = (-(3.0 * F[0]) + 4.0 * F[1] - F[2]) * res;
+      for (int o = 1; o <= n - 1; ++o) D[o] = (-F[o - 1] + F[o + 1]) * res;
+      D[n] = (3.0 * F[n] - 4.0 * F[n - 1] + F[n - 2]) * res;
+    }
+  }
+  h->tables.assign((size_t)T_COUNT * n2, 0.0);
+  auto TB = [&](int t, size_t q) -> double& { return h->tables[(size_t)t * n2 + q]; };
+  const double m2 = h->p.m * h->p.m;
+  for (size_t q = 0; q < n2; ++q) {
+    TB(T_ALPHA, q) = alpha[q];
+    TB(T_BETA, q) = beta[q];
+    TB(T_DXBETA, q) = dxbeta[q];
+    TB(T_SQRTG, q) = sqrtg[q];
+    TB(T_GRR, q) = h->gam[0 * n2 + q];
+    TB(T_GRP, q) = h->gam[2 * n2 + q];
+    TB(T_GTT, q) = h->gam[4 * n2 + q];
+    TB(T_GPP, q) = h->gam[8 * n2 + q];
+  }
+  (void)m2;
+}
+
+// derived products kept exactly as the reference groups them
+void derive_tables(kg_solver* h) {
+  const size_t n2 = (size_t)h->NI * h->NJ;
+  auto TB = [&](int t, size_t q) -> double& { return h->tables[(size_t)t * n2 + q]; };
+  const double m2 = h->p.m * h->p.m;
+  for (size_t q = 0; q < n2; ++q) {
+    const double asg = TB(T_ALPHA, q) * TB(T_SQRTG, q);
+    TB(T_ASG, q) = asg;
+    TB(T_ASG_GTT, q) = asg * TB(T_GTT, q);
+    TB(T_ASG_GRR, q) = asg * TB(T_GRR, q);
+    TB(T_A_GPP, q) = TB(T_ALPHA, q) * TB(T_GPP, q);
+    TB(T_AM2, q) = TB(T_ALPHA, q) * m2;
+  }
+}
+
+int upload_tables(kg_solver* h) {
+  const size_t n2 = (size_t)h->NI * h->NJ;
+  derive_tables(h);
+  KG_CK(cudaMemcpy2DAsync(h->dmet, sizeof(double) * h->PI, h->tables.data(), sizeof(double) * h->NI,
+                          sizeof(double) * h->NI, (size_t)T_COUNT * h->NJ, cudaMemcpyHostToDevice, h->stream));
+  (void)n2;
+  return KG_OK;
+}
+
+Metric metric_of(const kg_solver* h) {
+  Metric m;
+  const size_t tp = (size_t)h->NJ * h->PI;
+  const double* b = h->dmet;
+  m.alpha = b + T_ALPHA * tp;
+  m.beta = b + T_BETA * tp;
+  m.dxbeta = b + T_DXBETA * tp;
+  m.sqrtg = b + T_SQRTG * tp;
+  m.asg = b + T_ASG * tp;
+  m.grr = b + T_GRR * tp;
+  m.grp = b + T_GRP * tp;
+  m.gpp = b + T_GPP * tp;
+  m.asg_gtt = b + T_ASG_GTT * tp;
+  m.asg_grr = b + T_ASG_GRR * tp;
+  m.a_gpp = b + T_A_GPP * tp;
+  m.am2 = b + T_AM2 * tp;
+  m.gtt = b + T_GTT * tp;
+  return m;
+}
+
+// associated Legendre P_l^m with the Condon-Shortley phase (the convention of
+// GSL's gsl_sf_legendre_Plm used by tools/FFT_sph.f90:323): upward recurrence
+double plm(int l, int m, double x) {
+  double pmm = 1.0;
+  if (m > 0) {
+    const double somx2 = std::sqrt((1.0 - x) * (1.0 + x));
+    double fact = 1.0;
+    for (int i = 1; i <= m; ++i) {
+      pmm *= -fact * somx2;
+      fact += 2.0;
+    }
+  }
+  if (l == m) return pmm;
+  double pmmp1 = x * (2.0 * m + 1.0) * pmm;
+  if (l == m + 1) return pmmp1;
+  double pll = 0.0;
+  for (int ll = m + 2; ll <= l; ++ll) {
+    pll = (x * (2.0 * ll - 1.0) * pmmp1 - (ll + m - 1.0) * pmm) / (double)(ll - m);
+    pmm = pmmp1;
+    pmmp1 = pll;
+  }
+  return pll;
+}
+
+// norm * Plm of sph_harmonics (tools/FFT_sph.f90:306-324), incl. the pole rule
+double norm_plm(int l, int m, double theta) {
+  const double pi = std::acos(-1.0);
+  const double fact = std::sqrt((2.0 * l + 1.0) / (4.0 * pi));
+  double norm = fact;
+  if (m > 0)
+    for (int i = 1; i <= 2 * m; ++i) norm = norm / std::sqrt((double)(l - m + i));
+  const double x = std::cos(theta);
+  const double P = (std::fabs(x) > 0.9999) ? (m == 0 ? fact : 0.0) : plm(l, m, x);
+  return norm * P;
+}
+
+// detectors (MoL/diagnostic_lib.f90:124-134, main/global_numbers.f90:152-164)
+// and the domain_to_sph index search (tools/FFT_sph.f90:553-613)
+int build_detectors(kg_solver* h) {
+  const int n = h->n_det, Ny = h->Ny, Nz = h->Nz, L = h->L;
+  h->r_det.assign(n, 0.0);
+  h->index_det.assign(n, 0);
+  h->active.assign(n, 0);
+  h->r_det[0] = (1.0 + std::sqrt(1.0 - h->p.a * h->p.a));
+  h->r_det[n - 1] = h->p.xmax * 0.99;
+  for (int d = 2; d <= n - 1; ++d)
+    h->r_det[d - 1] = h->r_det[0] + (h->r_det[n - 1] - h->r_det[0]) / (double)n * (double)(d - 1);
+  auto rv = [&](int iv) { return h->xmin + (double)(iv - 1) * h->dx; };
+  for (int d = 0; d < n; ++d) {
+    for (int i = 1; i <= h->Nx - 1; ++i)
+      if (rv(i) <= h->r_det[d] && h->r_det[d] <= rv(i + 1)) {
+        h->index_det[d] = i;
+        break;
+      }
+    h->active[d] = (rv(1) <= h->r_det[d] && rv(h->Nx) > h->r_det[d] && h->index_det[d] > 0) ? 1 : 0;
+  }
+  // index search with the reference's arithmetic, per direction
+  const int b1l = -2, b1r = h->Nx + 2, b2l = -2, b2r = h->Ny + 2, b3l = 0, b3r = h->Nz;
+  auto RD = [&](int i) { return h->x1d[i - b1l]; };
+  auto TD = [&](int j) { return h->y1d[j - b2l]; };
+  auto PD = [&](int k) { return (double)k * h->dz; };
+  const double rmin = RD(b1l), dr = RD(b1l + 1) - RD(b1l);
+  const double thetamin = TD(b2l), dth = std::fabs(TD(b2l + 1) - TD(b2l));
+  const double phimin = PD(b3l), dph = std::fabs(PD(b3l + 1) - PD(b3l));
+  std::vector<int> i_r(n), i_th(Ny), th_flag(Ny), i_ph(Nz);
+  std::vector<double> w_r(n), w_th(Ny), w_ph(Nz), sint(Ny);
+  for (int d = 0; d < n; ++d) {
+    const double rr = rv(h->index_det[d] > 0 ? h->index_det[d] : 1);
+    int ir = (int)((rr - rmin) / dr) + b1l;
+    if (ir < b1l) ir = b1l;
+    if (ir > b1r - 1) ir = b1r - 1;
+    while (ir < b1r - 1 && rr >= RD(ir + 1)) ir++;
+    while (ir > b1l && rr < RD(ir)) ir--;
+    i_r[d] = ir - b1l;
+    w_r[d] = (rr - RD(ir)) / dr;
+  }
+  for (int jv = 1; jv <= Ny; ++jv) {
+    const double tt = (double)(jv - 1) * h->dy;
+    int it = (int)((tt - thetamin) / dth) + b2l;
+    if (it < b2l) it = b2l;
+    if (it > b2r - 1) it = b2r - 1;
+    while (it < b2r - 1 && tt >= TD(it + 1)) it++;
+    while (it > b2l && tt < TD(it)) it--;
+    i_th[jv - 1] = it - b2l;
+    w_th[jv - 1] = (tt - TD(it)) / dth;
+    th_flag[jv - 1] = (tt <= thetamin) ? 1 : (tt >= thetamin + dth * (double)(b2r - b2l)) ? 2 : 0;
+    sint[jv - 1] = std::sin(tt);
+  }
+  for (int kv = 1; kv <= Nz; ++kv) {
+    const double pp = (double)(kv - 1) * h->dz;
+    int ip = (int)((pp - phimin) / dph) + b3l;
+    if (ip < b3l) ip = b3l;
+    if (ip > b3r - 1) ip = b3r - 1;
+    while (ip < b3r - 1 && pp >= PD(ip + 1)) ip++;
+    while (ip > b3l && pp < PD(ip)) ip--;
+    i_ph[kv - 1] = ip;
+    w_ph[kv - 1] = (pp - PD(ip)) / dph;
+  }
+  // Y_lm factors: normP[l][m][jv], cos/sin(m phi_kv)
+  std::vector<double> normP((size_t)(L + 1) * (L + 1) * Ny, 0.0), cosm((size_t)(L + 1) * Nz), sinm((size_t)(L + 1) * Nz);
+  for (int l = 0; l <= L; ++l)
+    for (int m = 0; m <= l; ++m)
+      for (int jv = 1; jv <= Ny; ++jv) normP[((size_t)l * (L + 1) + m) * Ny + jv - 1] = norm_plm(l, m, (double)(jv - 1) * h->dy);
+  for (int m = 0; m <= L; ++m)
+    for (int kv = 1; kv <= Nz; ++kv) {
+      const double ph = (double)(kv - 1) * h->dz;
+      cosm[(size_t)m * Nz + kv - 1] = std::cos(m * ph);
+      sinm[(size_t)m * Nz + kv - 1] = std::sin(m * ph);
+    }
+  // device copies
+  const size_t nint = 2 * (size_t)n + 2 * (size_t)Ny + Nz;
+  const size_t ndbl = (size_t)n + 2 * (size_t)Ny + Nz + normP.size() + cosm.size() + sinm.size();
+  int rc;
+  if ((rc = dalloc(h, (void**)&h->d_int, nint * sizeof(int)))) return rc;
+  if ((rc = dalloc(h, (void**)&h->d_dbl, ndbl * sizeof(double)))) return rc;
+  std::vector<int> hi;
+  hi.insert(hi.end(), h->active.begin(), h->active.end());
+  hi.insert(hi.end(), i_r.begin(), i_r.end());
+  hi.insert(hi.end(), i_th.begin(), i_th.end());
+  hi.insert(hi.end(), th_flag.begin(), th_flag.end());
+  hi.insert(hi.end(), i_ph.begin(), i_ph.end());
+  std::vector<double> hd;
+  hd.insert(hd.end(), w_r.begin(), w_r.end());
+  hd.insert(hd.end(), w_th.begin(), w_th.end());
+  hd.insert(hd.end(), w_ph.begin(), w_ph.end());
+  hd.insert(hd.end(), sint.begin(), sint.end());
+  hd.insert(hd.end(), normP.begin(), normP.end());
+  hd.insert(hd.end(), cosm.begin(), cosm.end());
+  hd.insert(hd.end(), sinm.begin(), sinm.end());
+  KG_CK(cudaMemcpy(h->d_int, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice));
+  KG_CK(cudaMemcpy(h->d_dbl, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice));
+  const int* ip = h->d_int;
+  h->si.active = ip;
+  h->si.i_r = ip + n;
+  h->si.i_th = ip + 2 * n;
+  h->si.th_flag = ip + 2 * n + Ny;
+  h->si.i_ph = ip + 2 * n + 2 * Ny;
+  const double* dp = h->d_dbl;
+  h->si.w_r = dp;
+  h->si.w_th = dp + n;
+  h->si.w_ph = dp + n + Ny;
+  h->sint = dp + n + Ny + Nz;
+  h->normP = h->sint + Ny;
+  h->cosm = h->normP + normP.size();
+  h->sinm = h->cosm + cosm.size();
+  if ((rc = dalloc(h, (void**)&h->shells, (size_t)n * 4 * Ny * Nz * sizeof(double2)))) return rc;
+  if ((rc = dalloc(h, (void**)&h->alm, (size_t)(L + 1) * (2 * L + 1) * n * sizeof(double2)))) return rc;
+  if ((rc = dalloc(h, (void**)&h->flux, (size_t)3 * n * sizeof(double)))) return rc;
+  return KG_OK;
+}
+
+int ensure(kg_solver* h, double2** buf, int nslots) {
+  if (*buf) return KG_OK;
+  return dalloc(h, (void**)buf, (size_t)nslots * field_bytes(h));
+}
+
+int ensure_staging(kg_solver* h) {
+  if (h->stage_buf) return KG_OK;
+  const size_t plane_bytes = (size_t)5 * h->NI * h->NJ * sizeof(double2);
+  size_t want = (size_t)256 << 20;
+  int planes = (int)(want / plane_bytes);
+  if (planes < 1) planes = 1;
+  if (planes > h->NK) planes = h->NK;
+  h->stage_planes = planes;
+  h->stage_bytes = (size_t)planes * plane_bytes;
+  return dalloc(h, (void**)&h->stage_buf, h->stage_bytes);
+}
+
+// pointer to the 5-variable view of state `which`, or the Pi slot adjustments
+struct View {
+  double2* v[5];
+};
+
+int state_view(kg_solver* h, int which, View* out) {
+  int rc;
+  const Grid& g = h->g;
+  switch (which) {
+    case 0:
+      for (int v = 0; v < 5; ++v) out->v[v] = fld(h->U, g, v);
+      return KG_OK;
+    case 1:
+      if ((rc = ensure(h, &h->S, 6))) return rc;
+      for (int v = 0; v < 4; ++v) out->v[v] = fld(h->S, g, v);
+      out->v[4] = fld(h->S, g, h->s_cur);
+      return KG_OK;
+    case 2:
+      if ((rc = ensure(h, &h->T, 6))) return rc;
+      for (int v = 0; v < 4; ++v) out->v[v] = fld(h->T, g, v);
+      out->v[4] = fld(h->T, g, h->t_cur);
+      return KG_OK;
+    case 3:
+      if ((rc = ensure(h, &h->UP, 5))) return rc;
+      for (int v = 0; v < 5; ++v) out->v[v] = fld(h->UP, g, v);
+      return KG_OK;
+    default:
+      return set_err(h, KG_EINVAL, "state index must be 0..3");
+  }
+}
+
+// copy a Fortran-layout state (host or device memory) into 5 device planes
+int load_view(kg_solver* h, const View& V, const double* src, cudaMemcpyKind kind) {
+  int rc;
+  if ((rc = ensure_staging(h))) return rc;
+  const Grid& g = h->g;
+  const size_t plane_elems = (size_t)5 * h->NI * h->NJ;
+  // contiguous 5-variable device view? (slots 0..4 of one buffer)
+  for (int k0 = 0; k0 < h->NK; k0 += h->stage_planes) {
+    const int k1 = (k0 + h->stage_planes < h->NK) ? k0 + h->stage_planes : h->NK;
+    const size_t n = (size_t)(k1 - k0) * plane_elems;
+    KG_CK(cudaMemcpyAsync(h->stage_buf, (const double2*)src + (size_t)k0 * plane_elems, n * sizeof(double2), kind,
+                          h->stream));
+    // convert into a temporary contiguous 5-slot view if the slots are not contiguous
+    bool contiguous = true;
+    for (int v = 1; v < 5; ++v) contiguous = contiguous && (V.v[v] == V.v[0] + (long long)v * g.fs);
+    if (contiguous) {
+      { Prof pf(h, PK_CONVERT, 1); kg::launch_aos_to_soa(g, h->stage_buf, V.v[0], k0, k1, h->stream); }
+    } else {
+      // slot 4 lives elsewhere: convert variables 0..3 in place and variable 4 via its own base
+      // (aos_to_soa writes v*fs offsets from the base, so run it on a base that puts
+      // variable 4 at V.v[4]: write 0..4 at V.v[0], then move slot 4)
+      { Prof pf(h, PK_CONVERT, 1); kg::launch_aos_to_soa(g, h->stage_buf, V.v[0], k0, k1, h->stream); }
+      KG_CK(cudaMemcpyAsync(V.v[4] + (long long)k0 * g.plane, V.v[0] + 4 * g.fs + (long long)k0 * g.plane,
+                            (size_t)(k1 - k0) * g.plane * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    }
+    KG_CK(cudaGetLastError());
+  }
+  return KG_OK;
+}
+
+int store_view(kg_solver* h, const View& V, double* dst, cudaMemcpyKind kind) {
+  int rc;
+  if ((rc = ensure_staging(h))) return rc;
+  const Grid& g = h->g;
+  const size_t plane_elems = (size_t)5 * h->NI * h->NJ;
+  bool contiguous = true;
+  for (int v = 1; v < 5; ++v) contiguous = contiguous && (V.v[v] == V.v[0] + (long long)v * g.fs);
+  for (int k0 = 0; k0 < h->NK; k0 += h->stage_planes) {
+    const int k1 = (k0 + h->stage_planes < h->NK) ? k0 + h->stage_planes : h->NK;
+    const size_t n = (size_t)(k1 - k0) * plane_elems;
+    if (!contiguous) {
+      // gather slot 4 next to 0..3 (slot 4 of the same buffer is free scratch for S/T)
+      KG_CK(cudaMemcpyAsync(V.v[0] + 4 * g.fs + (long long)k0 * g.plane, V.v[4] + (long long)k0 * g.plane,
+                            (size_t)(k1 - k0) * g.plane * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    }
+    { Prof pf(h, PK_CONVERT, 1); kg::launch_soa_to_aos(g, V.v[0], h->stage_buf, k0, k1, h->stream); }
+    KG_CK(cudaGetLastError());
+    KG_CK(cudaMemcpyAsync((double2*)dst + (size_t)k0 * plane_elems, h->stage_buf, n * sizeof(double2), kind,
+                          h->stream));
+  }
+  return KG_OK;
+}
+
+void run_stage(kg_solver* h, int kind, const kg::StageLaunch& L) {
+  Prof pf(h, kind, 1);
+  kg::launch_stage(kind, L, h->stream);
+}
+void run_ghost(kg_solver* h, double2* u, const double2* up, int inflow) {
+  Prof pf(h, PK_GHOST, 2);
+  kg::launch_ghost_fill(h->g, u, up, inflow, h->stream);
+}
+
+kg::StageLaunch base_launch(kg_solver* h) {
+  kg::StageLaunch L;
+  memset(&L, 0, sizeof(L));
+  L.g = h->g;
+  L.m = metric_of(h);
+  L.metric_kind = h->p.metric == KG_SCHW_EF ? kg::MK_SCHW : kg::MK_KS;
+  return L;
+}
+
+void set_in(kg::StageLaunch& L, const Grid& g, double2* b0, double2* b4) {
+  for (int v = 0; v < 4; ++v) L.in[v] = fld(b0, g, v);
+  L.in[4] = b4;
+}
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+int kg_create(const kg_params* p, int device, kg_solver** out) {
+  if (!p || !out) return KG_EINVAL;
+  *out = nullptr;
+  if (p->g_pts != 2 || p->Nx < 4 || p->Ny < 5 || p->Nz < 5 || !(p->xmax > p->xmin) || !(p->CFL > 0.0) ||
+      (p->metric != KG_KERR_SCHILD && p->metric != KG_SCHW_EF) ||
+      (p->bc_rmax != KG_OUTFLOW && p->bc_rmax != KG_INFLOW) || p->l_max < 0 || p->l_max > 128)
+    return KG_EINVAL;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return KG_ENODEV;
+  }
+  if (device >= 0) {
+    if (device >= ndev || cudaSetDevice(device) != cudaSuccess) return KG_ENODEV;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || prop.major < 10) return KG_ENODEV;
+  kg_solver* h = new kg_solver();
+  h->p = *p;
+  h->device = dev;
+  h->Nx = p->Nx; h->Ny = p->Ny; h->Nz = p->Nz;
+  h->NI = p->Nx + 5; h->NJ = p->Ny + 5; h->NK = p->Nz + 1;
+  h->PI = (h->NI + 7) / 8 * 8;
+  h->n_det = p->n_det < 2 ? 2 : p->n_det;
+  h->L = p->l_max;
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return KG_ECUDA;
+  }
+  build_geometry(h);
+  Grid& g = h->g;
+  g.NI = h->NI; g.NJ = h->NJ; g.NK = h->NK; g.PI = h->PI;
+  g.plane = (long long)h->NJ * h->PI;
+  g.fs = (long long)h->NK * g.plane;
+  g.Nz = h->Nz; g.dis = h->Nz / 2; g.Nzm1 = h->Nz - 1;
+  g.rdx = 0.50 / h->dx; g.rdy = 0.50 / h->dy; g.rdz = 0.50 / h->dz;
+  g.dt = h->dt;
+  int rc = KG_OK;
+  if ((rc = dalloc(h, (void**)&h->dmet, (size_t)T_COUNT * h->NJ * h->PI * sizeof(double))) ||
+      (rc = upload_tables(h)) || (rc = dalloc(h, (void**)&h->U, 5 * field_bytes(h))) ||
+      (rc = dalloc(h, (void**)&h->partials, (size_t)(kg::mass_blocks(g) + 1) * sizeof(double))) ||
+      (rc = build_detectors(h))) {
+    kg_destroy(h);
+    return rc;
+  }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    kg_destroy(h);
+    return KG_ECUDA;
+  }
+  *out = h;
+  return KG_OK;
+}
+
+int kg_destroy(kg_solver* h) {
+  if (!h) return KG_EINVAL;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  void* bufs[] = {h->dmet, h->U, h->S, h->T, h->RK, h->UP, h->HV, h->stage_buf, h->rho, h->partials,
+                  h->d_int, h->d_dbl, h->shells, h->alm, h->flux};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  for (auto& r : h->recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : h->pool) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return KG_OK;
+}
+
+const char* kg_last_error(const kg_solver* h) { return h ? h->err.c_str() : "null handle"; }
+
+int kg_get_scalars(const kg_solver* h, double* o) {
+  if (!h || !o) return KG_EINVAL;
+  o[0] = h->dx; o[1] = h->dy; o[2] = h->dz; o[3] = h->dt; o[4] = h->t;
+  o[5] = h->xmin; o[6] = h->xmax; o[7] = (double)h->Nt; o[8] = h->r_max;
+  return KG_OK;
+}
+
+int kg_set_time(kg_solver* h, double t) {
+  if (!h) return KG_EINVAL;
+  h->t = t;
+  return KG_OK;
+}
+
+int kg_set_dt(kg_solver* h, double dt) {
+  if (!h || !(dt > 0.0)) return KG_EINVAL;
+  h->dt = dt;
+  h->g.dt = dt;
+  return KG_OK;
+}
+
+void* kg_get_stream(const kg_solver* h) { return h ? (void*)h->stream : nullptr; }
+size_t kg_device_bytes(const kg_solver* h) { return h ? h->bytes : 0; }
+
+int kg_synchronize(kg_solver* h) {
+  if (!h) return KG_EINVAL;
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
+int kg_set_state(kg_solver* h, int which, const double* host_u) {
+  if (!h || !host_u) return KG_EINVAL;
+  View V;
+  int rc;
+  if ((rc = state_view(h, which, &V))) return rc;
+  if ((rc = load_view(h, V, host_u, cudaMemcpyHostToDevice))) return rc;
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
+int kg_get_state(kg_solver* h, int which, double* host_u) {
+  if (!h || !host_u) return KG_EINVAL;
+  View V;
+  int rc;
+  if ((rc = state_view(h, which, &V))) return rc;
+  if ((rc = store_view(h, V, host_u, cudaMemcpyDeviceToHost))) return rc;
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
+int kg_set_state_device(kg_solver* h, int which, const double* dev_u) {
+  if (!h || !dev_u) return KG_EINVAL;
+  View V;
+  int rc;
+  if ((rc = state_view(h, which, &V))) return rc;
+  return load_view(h, V, dev_u, cudaMemcpyDeviceToDevice);
+}
+
+int kg_get_state_device(kg_solver* h, int which, double* dev_u) {
+  if (!h || !dev_u) return KG_EINVAL;
+  View V;
+  int rc;
+  if ((rc = state_view(h, which, &V))) return rc;
+  return store_view(h, V, dev_u, cudaMemcpyDeviceToDevice);
+}
+
+int kg_pirk2(kg_solver* h, int nsteps) {
+  if (!h || nsteps < 0) return KG_EINVAL;
+  int rc;
+  if ((rc = ensure(h, &h->S, 6))) return rc;
+  const Grid& g = h->g;
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  for (int s = 0; s < nsteps; ++s) {
+    double2* Sold = fld(h->S, g, h->s_cur);
+    double2* Snew = fld(h->S, g, 9 - h->s_cur);
+    kg::StageLaunch L = base_launch(h);
+    set_in(L, g, h->U, fld(h->U, g, 4));
+    L.base = h->U;
+    L.out = h->S;
+    run_stage(h, kg::ST_P2_S1A, L);
+    set_in(L, g, h->S, Sold);
+    L.out4 = Snew;
+    run_stage(h, kg::ST_P2_S1B, L);
+    set_in(L, g, h->S, Snew);
+    L.out = h->U;
+    L.skip_last_i = inflow;
+    run_stage(h, kg::ST_P2_S2, L);
+    run_ghost(h, h->U, h->U, inflow);
+    h->s_cur = 9 - h->s_cur;
+    h->t = h->t + h->dt;
+  }
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
+int kg_pirk3(kg_solver* h, int nsteps) {
+  if (!h || nsteps < 0) return KG_EINVAL;
+  int rc;
+  if ((rc = ensure(h, &h->S, 6)) || (rc = ensure(h, &h->T, 6))) return rc;
+  const Grid& g = h->g;
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  for (int s = 0; s < nsteps; ++s) {
+    double2* Sold = fld(h->S, g, h->s_cur);
+    double2* Snew = fld(h->S, g, 9 - h->s_cur);
+    double2* Told = fld(h->T, g, h->t_cur);
+    double2* Tnew = fld(h->T, g, 9 - h->t_cur);
+    kg::StageLaunch L = base_launch(h);
+    set_in(L, g, h->U, fld(h->U, g, 4));
+    L.base = h->U;
+    L.out = h->S;
+    run_stage(h, kg::ST_P2_S1A, L);
+    set_in(L, g, h->S, Sold);
+    L.out4 = Snew;
+    run_stage(h, kg::ST_P2_S1B, L);
+    set_in(L, g, h->S, Snew);
+    L.out = h->T;
+    run_stage(h, kg::ST_P3_S2A, L);
+    set_in(L, g, h->T, Told);
+    L.aux4 = Snew;
+    L.out4 = Tnew;
+    run_stage(h, kg::ST_P3_S2B, L);
+    set_in(L, g, h->T, Tnew);
+    L.out = h->U;
+    L.skip_last_i = inflow;
+    run_stage(h, kg::ST_P3_S3, L);
+    run_ghost(h, h->U, h->U, inflow);
+    h->s_cur = 9 - h->s_cur;
+    h->t_cur = 9 - h->t_cur;
+    h->t = h->t + h->dt;
+  }
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
+int kg_rk3(kg_solver* h, int nsteps) {
+  if (!h || nsteps < 0) return KG_EINVAL;
+  int rc;
+  if ((rc = ensure(h, &h->RK, 15))) return rc;
+  const Grid& g = h->g;
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  double2* R1 = h->RK;
+  double2* R2 = fld(h->RK, g, 5);
+  for (int s = 0; s < nsteps; ++s) {
+    kg::StageLaunch L = base_launch(h);
+    L.base = h->U;
+    set_in(L, g, h->U, fld(h->U, g, 4));
+    L.out = R1;
+    run_stage(h, kg::ST_RK3_1, L);
+    run_ghost(h, R1, h->U, inflow);
+    set_in(L, g, R1, fld(R1, g, 4));
+    L.out = R2;
+    run_stage(h, kg::ST_RK3_2, L);
+    run_ghost(h, R2, h->U, inflow);
+    set_in(L, g, R2, fld(R2, g, 4));
+    L.out = h->U;
+    L.skip_last_i = inflow;
+    run_stage(h, kg::ST_RK3_3, L);
+    run_ghost(h, h->U, h->U, inflow);
+    h->t = h->t + h->dt;
+  }
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
+int kg_rk4(kg_solver* h, int nsteps) {
+  if (!h || nsteps < 0) return KG_EINVAL;
+  int rc;
+  if ((rc = ensure(h, &h->RK, 15))) return rc;
+  const Grid& g = h->g;
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  double2* R1 = h->RK;
+  double2* R2 = fld(h->RK, g, 5);
+  double2* A = fld(h->RK, g, 10);
+  for (int s = 0; s < nsteps; ++s) {
+    kg::StageLaunch L = base_launch(h);
+    L.base = h->U;
+    L.acc = A;
+    set_in(L, g, h->U, fld(h->U, g, 4));
+    L.out = R1;
+    run_stage(h, kg::ST_RK4_1, L);
+    run_ghost(h, R1, h->U, inflow);
+    set_in(L, g, R1, fld(R1, g, 4));
+    L.out = R2;
+    run_stage(h, kg::ST_RK4_2, L);
+    run_ghost(h, R2, h->U, inflow);
+    set_in(L, g, R2, fld(R2, g, 4));
+    L.out = R1;
+    run_stage(h, kg::ST_RK4_3, L);
+    run_ghost(h, R1, h->U, inflow);
+    set_in(L, g, R1, fld(R1, g, 4));
+    L.out = h->U;
+    L.skip_last_i = inflow;
+    run_stage(h, kg::ST_RK4_4, L);
+    run_ghost(h, h->U, h->U, inflow);
+    h->t = h->t + h->dt;
+  }
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
+int kg_rhs(kg_solver* h, const double* host_vars, double* host_rhs, unsigned mask) {
+  if (!h || !host_vars || !host_rhs) return KG_EINVAL;
+  int rc;
+  if ((rc = ensure(h, &h->HV, 10))) return rc;
+  const Grid& g = h->g;
+  View Vin, Vout;
+  for (int v = 0; v < 5; ++v) {
+    Vin.v[v] = fld(h->HV, g, v);
+    Vout.v[v] = fld(h->HV, g, 5 + v);
+  }
+  if ((rc = load_view(h, Vin, host_vars, cudaMemcpyHostToDevice))) return rc;
+  if ((rc = load_view(h, Vout, host_rhs, cudaMemcpyHostToDevice))) return rc;
+  const double2* in[5];
+  for (int v = 0; v < 5; ++v) in[v] = Vin.v[v];
+  Prof pf(h, PK_RHS, 1);
+  kg::launch_rhs(g, metric_of(h), h->p.metric == KG_SCHW_EF ? kg::MK_SCHW : kg::MK_KS, in, Vout.v[0], mask,
+                 h->stream);
+  KG_CK(cudaGetLastError());
+  if ((rc = store_view(h, Vout, host_rhs, cudaMemcpyDeviceToHost))) return rc;
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
+int kg_boundary(kg_solver* h, unsigned mask) {
+  if (!h) return KG_EINVAL;
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  const double2* up = h->UP ? h->UP : h->U;
+  for (int f = 0; f < 6; ++f)
+    if (mask & (1u << f)) {
+      Prof pf(h, PK_FACE, 1);
+      kg::launch_face(h->g, h->U, up, inflow, f, h->stream);
+    }
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
+int kg_send_recv(kg_solver* h) { return h ? KG_OK : KG_EINVAL; }
+
+int kg_get_metric(kg_solver* h, double* out8) {
+  if (!h || !out8) return KG_EINVAL;
+  const size_t n2 = (size_t)h->NI * h->NJ;
+  const int order[8] = {T_ALPHA, T_BETA, T_DXBETA, T_SQRTG, T_GRR, T_GRP, T_GTT, T_GPP};
+  for (int t = 0; t < 8; ++t)
+    KG_CK(cudaMemcpy2DAsync(out8 + t * n2, sizeof(double) * h->NI, h->dmet + (size_t)order[t] * h->NJ * h->PI,
+                            sizeof(double) * h->PI, sizeof(double) * h->NI, h->NJ, cudaMemcpyDeviceToHost,
+                            h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
+int kg_set_metric(kg_solver* h, const double* in8) {
+  if (!h || !in8) return KG_EINVAL;
+  const size_t n2 = (size_t)h->NI * h->NJ;
+  const int order[8] = {T_ALPHA, T_BETA, T_DXBETA, T_SQRTG, T_GRR, T_GRP, T_GTT, T_GPP};
+  for (int t = 0; t < 8; ++t) memcpy(h->tables.data() + (size_t)order[t] * n2, in8 + t * n2, n2 * sizeof(double));
+  int rc;
+  if ((rc = upload_tables(h))) return rc;
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
+int kg_validate_inverse_metric(kg_solver* h, int* e4, int* e3) {
+  if (!h) return KG_EINVAL;
+  const size_t n2 = (size_t)h->NI * h->NJ;
+  const double tol = 1.0e-10;
+  long a4 = 0, a3 = 0;
+  for (size_t q = 0; q < n2; ++q) {
+    for (int mu = 0; mu < 4; ++mu)
+      for (int la = 0; la < 4; ++la) {
+        double d = 0.0;
+        for (int nu = 0; nu < 4; ++nu) d = d + h->gdn[(mu * 4 + nu) * n2 + q] * h->gup[(nu * 4 + la) * n2 + q];
+        if (mu == la ? std::fabs(d - 1.0) > tol : std::fabs(d) > tol) a4++;
+      }
+    for (int mu = 1; mu < 4; ++mu)
+      for (int la = 1; la < 4; ++la) {
+        double d = 0.0;
+        for (int nu = 1; nu < 4; ++nu) d = d + h->gdn[(mu * 4 + nu) * n2 + q] * h->gam[((nu - 1) * 3 + la - 1) * n2 + q];
+        if (mu == la ? std::fabs(d - 1.0) > tol : std::fabs(d) > tol) a3++;
+      }
+  }
+  if (e4) *e4 = (int)(a4 * h->NK);
+  if (e3) *e3 = (int)(a3 * h->NK);
+  return KG_OK;
+}
+
+int kg_density(kg_solver* h) {
+  if (!h) return KG_EINVAL;
+  if (!h->rho) {
+    int rc = dalloc(h, (void**)&h->rho, (size_t)h->g.fs * sizeof(double));
+    if (rc) return rc;
+  }
+  {
+    Prof pf(h, PK_DENSITY, 1);
+    kg::launch_density(h->g, metric_of(h), h->U, h->p.m * h->p.m, h->rho, h->stream);
+  }
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
+int kg_get_density(kg_solver* h, double* host_rho) {
+  if (!h || !host_rho) return KG_EINVAL;
+  if (!h->rho) return set_err(h, KG_ESTATE, "density has not been computed");
+  KG_CK(cudaMemcpy2DAsync(host_rho, sizeof(double) * h->NI, h->rho, sizeof(double) * h->PI, sizeof(double) * h->NI,
+                          (size_t)h->NJ * h->NK, cudaMemcpyDeviceToHost, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
+int kg_mass_scalar(kg_solver* h, double* out) {
+  if (!h || !out) return KG_EINVAL;
+  if (!h->rho) {
+    int rc = dalloc(h, (void**)&h->rho, (size_t)h->g.fs * sizeof(double));
+    if (rc) return rc;
+  }
+  double* res = h->partials + kg::mass_blocks(h->g);
+  {
+    Prof pf(h, PK_MASS, 2);
+    kg::launch_mass(h->g, metric_of(h), h->rho, h->dx * h->dy * h->dz, h->partials, res, h->stream);
+  }
+  KG_CK(cudaGetLastError());
+  KG_CK(cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
+int kg_currents_detectors(kg_solver* h, double* mom) {
+  if (!h || !mom) return KG_EINVAL;
+  {
+    Prof pf(h, PK_SHELL, __builtin_popcount(2 | 4 | 8));
+    kg::launch_shell_interp(h->g, metric_of(h), h->U, h->si, h->n_det, h->Ny, h->Nz, 2 | 4 | 8, h->shells, h->stream);
+  }
+  {
+    Prof pf(h, PK_FLUX, 1);
+    kg::launch_flux(h->shells, h->si.active, h->n_det, h->Ny, h->Nz, h->dy * h->dz, h->flux, h->stream);
+  }
+  KG_CK(cudaGetLastError());
+  std::vector<double> f(3 * (size_t)h->n_det);
+  KG_CK(cudaMemcpyAsync(f.data(), h->flux, f.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  for (int d = 0; d < h->n_det; ++d)
+    if (h->active[d])
+      for (int c = 0; c < 3; ++c) mom[c + 3 * d] = f[c + 3 * d];
+  return KG_OK;
+}
+
+int kg_proyector_detectors(kg_solver* h, double* host_alm) {
+  if (!h || !host_alm) return KG_EINVAL;
+  {
+    Prof pf(h, PK_SHELL, __builtin_popcount(1));
+    kg::launch_shell_interp(h->g, metric_of(h), h->U, h->si, h->n_det, h->Ny, h->Nz, 1, h->shells, h->stream);
+  }
+  {
+    Prof pf(h, PK_PROJECT, 1);
+    kg::launch_project(h->shells, h->si.active, h->n_det, h->L, h->Ny, h->Nz, h->normP, h->cosm, h->sinm, h->sint,
+                     h->dy * h->dz, h->alm, h->stream);
+  }
+  KG_CK(cudaGetLastError());
+  const size_t per = (size_t)(h->L + 1) * (2 * h->L + 1);
+  std::vector<double2> a(per * h->n_det);
+  KG_CK(cudaMemcpyAsync(a.data(), h->alm, a.size() * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  for (int d = 0; d < h->n_det; ++d)
+    if (h->active[d]) memcpy(host_alm + 2 * per * d, a.data() + per * d, per * sizeof(double2));
+  return KG_OK;
+}
+
+int kg_diagnostic(kg_solver* h, int index, double* mass_out) {
+  if (!h) return KG_EINVAL;
+  if (index % h->save == 0) {
+    {
+      Prof pf(h, PK_SHELL, __builtin_popcount(15));
+      kg::launch_shell_interp(h->g, metric_of(h), h->U, h->si, h->n_det, h->Ny, h->Nz, 15, h->shells, h->stream);
+    }
+    {
+      Prof pf(h, PK_FLUX, 1);
+      kg::launch_flux(h->shells, h->si.active, h->n_det, h->Ny, h->Nz, h->dy * h->dz, h->flux, h->stream);
+    }
+    {
+      Prof pf(h, PK_PROJECT, 1);
+      kg::launch_project(h->shells, h->si.active, h->n_det, h->L, h->Ny, h->Nz, h->normP, h->cosm, h->sinm, h->sint,
+                       h->dy * h->dz, h->alm, h->stream);
+    }
+    KG_CK(cudaGetLastError());
+  }
+  if (mass_out) return kg_mass_scalar(h, mass_out);
+  return KG_OK;
+}
+
+int kg_get_detectors(kg_solver* h, double* r_det, int* index_det) {
+  if (!h) return KG_EINVAL;
+  for (int d = 0; d < h->n_det; ++d) {
+    if (r_det) r_det[d] = h->r_det[d];
+    if (index_det) index_det[d] = h->index_det[d];
+  }
+  return KG_OK;
+}
+
+int kg_sph_harmonics(kg_solver* h, int L, double* out) {
+  if (!h || !out || L < 0) return KG_EINVAL;
+  const int NL = L + 1, NM = 2 * L + 1;
+  double2* Y = (double2*)out;
+  memset(Y, 0, sizeof(double2) * (size_t)NL * NM * h->Ny * h->Nz);
+  for (int l = 0; l <= L; ++l)
+    for (int m = 0; m <= l; ++m)
+      for (int jv = 1; jv <= h->Ny; ++jv) {
+        const double np = norm_plm(l, m, (double)(jv - 1) * h->dy);
+        for (int kv = 1; kv <= h->Nz; ++kv) {
+          const double ph = (double)(kv - 1) * h->dz;
+          const double2 y = make_double2(np * std::cos(m * ph), np * std::sin(m * ph));
+          const size_t base = (size_t)(jv - 1) + (size_t)h->Ny * (kv - 1);
+          Y[l + NL * ((m + L) + NM * base)] = y;
+          if (m > 0) {
+            const double sg = (m % 2) ? -1.0 : 1.0;
+            Y[l + NL * ((-m + L) + NM * base)] = make_double2(sg * y.x, sg * -y.y);
+          }
+        }
+      }
+  return KG_OK;
+}
+
+int kg_profile_enable(kg_solver* h, int on) {
+  if (!h) return KG_EINVAL;
+  h->prof_on = on ? 1 : 0;
+  return KG_OK;
+}
+
+int kg_profile_kinds(void) { return PK_COUNT; }
+
+const char* kg_profile_kind_name(int kind) { return (kind >= 0 && kind < PK_COUNT) ? kPkNames[kind] : ""; }
+
+int kg_profile_read(kg_solver* h, double* ms, long long* launches) {
+  if (!h) return KG_EINVAL;
+  KG_CK(cudaStreamSynchronize(h->stream));
+  if (ms)
+    for (int k = 0; k < PK_COUNT; ++k) ms[k] = 0.0;
+  if (launches)
+    for (int k = 0; k < PK_COUNT; ++k) launches[k] = 0;
+  for (auto& r : h->recs) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, r.a, r.b);
+    if (ms) ms[r.kind] += t;
+    if (launches) launches[r.kind] += 1;
+    h->pool.push_back(r.a);
+    h->pool.push_back(r.b);
+  }
+  h->recs.clear();
+  return KG_OK;
+}
+
+long long kg_launch_count(const kg_solver* h) { return h ? h->launches : 0; }
+
+}  // extern "C"

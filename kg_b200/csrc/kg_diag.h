@@ -1,0 +1,32 @@
+// kg_diag.h -- detector-shell tables and launchers of kg_diag.cu
+#pragma once
+#include <cuda_runtime.h>
+#include "kg_device.cuh"
+
+namespace kg {
+
+// Interpolation tables of domain_to_sph (tools/FFT_sph.f90:525-651) for the
+// detector shells, all device pointers.  Per detector: evolution-grid r index
+// (0-based ii) and weight; per vertex theta index jv: jj index, weight and a
+// pole flag (1: copy row 0, 2: copy row NJ-1); per vertex phi index kv: k
+// index and weight.
+struct ShellInterp {
+  const int* active;   // [n_det] detector inside the grid
+  const int* i_r;      // [n_det]
+  const double* w_r;   // [n_det]
+  const int* i_th;     // [Ny]
+  const double* w_th;  // [Ny]
+  const int* th_flag;  // [Ny]
+  const int* i_ph;     // [Nz]
+  const double* w_ph;  // [Nz]
+};
+
+void launch_shell_interp(const Grid& g, const Metric& m, const double2* u, const ShellInterp& si, int n_det, int Ny,
+                         int Nz, int which_mask, double2* out, cudaStream_t st);
+void launch_flux(const double2* shells, const int* active, int n_det, int Ny, int Nz, double dydz, double* out,
+                 cudaStream_t st);
+void launch_project(const double2* shells, const int* active, int n_det, int L, int Ny, int Nz, const double* normP,
+                    const double* cosm, const double* sinm, const double* sint, double dydz, double2* alm,
+                    cudaStream_t st);
+
+}  // namespace kg

@@ -1,0 +1,61 @@
+// kg_internal.h -- declarations shared by the translation units of
+// libkg_b200.so (not part of the public C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include "kg_device.cuh"
+
+namespace kg {
+
+// stage kinds of the fused RHS + combination kernel
+enum StageKind {
+  ST_P2_S1A = 0,  // PIRK stage 1, phi/psi part:   S(1:4) = u + dt*rhs(u)
+  ST_P2_S1B,      // PIRK stage 1, Pi part:        S(5)   = u(5) + dt*rhs_pi(S)
+  ST_P2_S2,       // PIRK2 stage 2:                u = 0.5*(u_p + S + dt*rhs(S))
+  ST_P3_S2A,      // PIRK3 stage 2, phi/psi part:  T(1:4) = 0.75 u_p + 0.25 (S + dt rhs(S))
+  ST_P3_S2B,      // PIRK3 stage 2, Pi part:       T(5)   = 0.75 u_p + 0.25 (S(5) + dt rhs_pi(T))
+  ST_P3_S3,       // PIRK3 stage 3:                u = 1/3 u_p + 2/3 (T + dt rhs(T))
+  ST_RK3_1,       // RK3 stage 1:                  S = u_p + rhs*dt
+  ST_RK3_2,       // RK3 stage 2:                  S' = 0.75 u_p + 0.25 (S + rhs*dt)
+  ST_RK3_3,       // RK3 stage 3:                  u = u_p/3 + 2 (S' + rhs*dt)/3
+  ST_RK4_1,       // RK4 stages: k = rhs*dt, accumulator k1 + 2k2 + 2k3
+  ST_RK4_2,
+  ST_RK4_3,
+  ST_RK4_4
+};
+
+struct StageLaunch {
+  Grid g;
+  Metric m;
+  int metric_kind;
+  const double2* in[5];
+  const double2* base;
+  const double2* aux4;
+  double2* out;
+  double2* out4;
+  double2* acc;
+  int skip_last_i;
+};
+
+void launch_stage(int kind, const StageLaunch& L, cudaStream_t st);
+void launch_rhs(const Grid& g, const Metric& m, int metric_kind, const double2* const in[5], double2* out,
+                unsigned mask, cudaStream_t st);
+
+// boundary fills on a 5-variable state u; up = u_p (inflow source)
+void launch_ghost_fill(const Grid& g, double2* u, const double2* up, int inflow, cudaStream_t st);
+void launch_face(const Grid& g, double2* u, const double2* up, int inflow, int face, cudaStream_t st);
+
+// layout conversion between the Fortran AoS layout and the device planes,
+// for planes [k0, k1) of all 5 variables; aos points at plane k0
+void launch_aos_to_soa(const Grid& g, const double2* aos, double2* soa, int k0, int k1, cudaStream_t st);
+void launch_soa_to_aos(const Grid& g, const double2* soa, double2* aos, int k0, int k1, cudaStream_t st);
+
+// diagnostics
+struct ShellInterp;  // per-detector interpolation tables (kg_diag.cu)
+void launch_density(const Grid& g, const Metric& m, const double2* u, double mass2, double* rho, cudaStream_t st);
+// trapezium integral of rho*sqrtg over i in [0,Nx], j in [0,Ny], k in [0,Nz];
+// partial sums in `partials` (>= nblocks doubles), result in *out (device)
+int mass_blocks(const Grid& g);
+void launch_mass(const Grid& g, const Metric& m, const double* rho, double dxdydz, double* partials,
+                 double* out, cudaStream_t st);
+
+}  // namespace kg

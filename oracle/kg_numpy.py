@@ -1,0 +1,298 @@
+"""Whole-array numpy restatement of the KG method-of-lines path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/ to cross-check the C oracle
+(oracle/kg_oracle.c) on small grids.  It is an independent transcription of
+the same Fortran statements, written in the array syntax the reference uses
+(every operator returns a full temporary), so that a transcription slip in
+either restatement shows up as a mismatch.
+
+Reference files (FlavioRosales/KG): tools/finite_differences.f90:17-44,
+193-239, 310-338, 767-801; MoL/lines_method_lib.f90:211-597, 671-753;
+MoL/geometry.f90:92-406; MoL/mesh_refinement_lib.f90:100-147;
+MoL/diagnostic_lib.f90:101-107.
+
+Arrays are indexed [i - iL, j - jL, k] with i = r (iL = -g), j = theta
+(jL = -g), k = phi (0..Nz).  Complex-by-real products are numpy's
+complex128 x float64, which agree bit for bit with the component-wise
+product for finite values.
+"""
+from __future__ import annotations
+
+import math
+import numpy as np
+
+
+class NumpyKG:
+    def __init__(self, Nx, Ny, Nz, xmin, xmax, CFL, m=0.0, a=0.0, M_bh=1.0,
+                 metric="Kerr_Schild", bc_rmax="outflow", tmin=0.0, tmax=1.0,
+                 g=2, dt_override=0.0):
+        self.Nx, self.Ny, self.Nz, self.g = Nx, Ny, Nz, g
+        self.m, self.a, self.M, self.metric, self.bc = m, a, M_bh, metric, bc_rmax
+        self.iL, self.iR, self.jL, self.jR, self.kL, self.kR = -g, Nx + g, -g, Ny + g, 0, Nz
+        self.NI, self.NJ, self.NK = Nx + 2 * g + 1, Ny + 2 * g + 1, Nz + 1
+        pi = math.acos(-1.0)
+        dxr = (xmax - xmin) / 1.0
+        self.xmin = xmin + 0.0 * dxr
+        self.xmax = xmin + 1.0 * dxr
+        self.dx = (self.xmax - self.xmin) / float(Nx)
+        self.dy = pi / float(Ny - 1)
+        self.dz = 2.0 * pi / float(Nz - 1)
+        i = np.arange(self.iL, self.iR + 1)
+        j = np.arange(self.jL, self.jR + 1)
+        self.x = self.xmin + (i + g).astype(np.float64) * self.dx
+        self.y = -self.dy / 2.0 + j.astype(np.float64) * self.dy
+        dxx = self.x[1] - self.x[0]
+        self.dt = CFL * min(dxx, math.exp(xmin) * self.dy, math.exp(xmin) * math.sin(self.dy / 2.0) * self.dz)
+        if dt_override > 0:
+            self.dt = dt_override
+        self.t = tmin
+        self._metric()
+        shape = (self.NI, self.NJ, self.NK)
+        self.u = np.zeros((5,) + shape, np.complex128)
+        self.u_p = np.zeros_like(self.u)
+        self.u_stage = np.zeros_like(self.u)
+        self.u_stage_2 = np.zeros_like(self.u)
+        self.rhs_u = np.zeros_like(self.u)
+
+    # ---- metric (MoL/geometry.f90) as 2-D (r, theta) arrays broadcast over phi
+    def _metric(self):
+        x = self.x[:, None] * np.ones((1, self.NJ))
+        y = np.ones((self.NI, 1)) * self.y[None, :]
+        M, A = self.M, self.a
+        gd = np.zeros((4, 4) + x.shape)
+        if self.metric == "Kerr_Schild":
+            c2 = np.cos(y) ** 2
+            s2 = np.sin(y) ** 2
+            gd[0, 0] = -1.0 + 2.0 * M * x / (x ** 2 + A ** 2 * c2)
+            gd[0, 1] = (2.0 * M * x / (x ** 2 + A ** 2 * c2))
+            gd[0, 3] = -(2.0 * A * M * x * s2 / (x ** 2 + A ** 2 * c2))
+            gd[1, 0] = gd[0, 1]
+            gd[1, 1] = (1.0 + 2.0 * M * x / (x ** 2 + A ** 2 * c2))
+            gd[1, 3] = (-(A * (1.0 + 2.0 * M * x / (x ** 2 + A ** 2 * c2)) * s2))
+            gd[2, 2] = (x ** 2 + A ** 2 * c2)
+            gd[3, 0] = gd[0, 3]
+            gd[3, 1] = gd[1, 3]
+            gd[3, 3] = ((A ** 2 + x ** 2) ** 2 - A ** 2 * (-(2.0 * M * x) + A ** 2 + x ** 2) * s2) * s2 / (x ** 2 + A ** 2 * c2)
+        else:
+            gd[0, 0] = -(1.0 - 2.0 * M / x)
+            gd[0, 1] = 2.0 * M / x
+            gd[1, 0] = gd[0, 1]
+            gd[1, 1] = 1.0 + 2.0 * M / x
+            gd[2, 2] = x ** 2
+            gd[3, 3] = x ** 2 * np.sin(y) ** 2
+        # boundary_theta_dn: last theta row from the one before
+        gd[:, :, :, -1] = gd[:, :, :, -2]
+        gd[0, 2, :, -1] = -gd[0, 2, :, -2]
+        gd[1, 2, :, -1] = -gd[1, 2, :, -2]
+        for (p, q) in ((1, 0), (2, 0), (3, 0), (2, 1), (3, 1), (3, 2)):
+            gd[p, q] = gd[q, p]
+        self.sqrtg = np.sqrt(gd[2, 2] * (gd[1, 1] * gd[3, 3] - gd[1, 3] ** 2))
+        g00, g01, g03, g11, g13, g22, g33 = gd[0, 0], gd[0, 1], gd[0, 3], gd[1, 1], gd[1, 3], gd[2, 2], gd[3, 3]
+        idetg = 1.0 / (((g33 * g11 - g13 ** 2) * g00 - g33 * g01 ** 2 + 2.0 * g13 * g03 * g01 - g11 * g03 ** 2) * g22)
+        gu = np.zeros_like(gd)
+        gu[0, 0] = g22 * (g11 * g33 - g13 ** 2) * idetg
+        gu[0, 1] = g22 * (g13 * g03 - g01 * g33) * idetg
+        gu[0, 3] = g22 * (g13 * g01 - g11 * g03) * idetg
+        gu[1, 1] = g22 * (g33 * g00 - g03 ** 2) * idetg
+        gu[1, 3] = g22 * (-g13 * g00 + g03 * g01) * idetg
+        gu[2, 2] = ((g33 * g11 - g13 ** 2) * g00 - g33 * g01 ** 2 + 2.0 * g13 * g03 * g01 - g11 * g03 ** 2) * idetg
+        gu[3, 3] = g22 * (g11 * g00 - g01 ** 2) * idetg
+        gu[:, :, :, -1] = gu[:, :, :, -2]
+        gu[0, 2, :, -1] = -gu[0, 2, :, -2]
+        gu[1, 2, :, -1] = -gu[1, 2, :, -2]
+        for (p, q) in ((1, 0), (2, 0), (3, 0), (2, 1), (3, 1), (3, 2)):
+            gu[p, q] = gu[q, p]
+        self.g_dn, self.g_up = gd, gu
+        self.alpha = np.sqrt(-1.0 / gu[0, 0])
+        self.beta = np.stack([self.alpha ** 2 * gu[0, i] for i in (1, 2, 3)])
+        self.gamma_up = np.zeros((3, 3) + x.shape)
+        for i in range(3):
+            for j in range(3):
+                self.gamma_up[i, j] = gu[i + 1, j + 1] + self.beta[i] * self.beta[j] / self.alpha ** 2
+        self.dx_beta = self.dx1(self.beta[0][:, :, None].astype(np.complex128), self.dx).real[:, :, 0]
+
+    def _b(self, t):  # broadcast a 2-D table over phi
+        return t[:, :, None]
+
+    @staticmethod
+    def cdiv(z, s):
+        """Component-wise complex / real quotient (numpy's complex division
+        multiplies by a reciprocal, which is not what gfortran emits)."""
+        out = np.empty(np.broadcast(z, s).shape, np.complex128)
+        out.real = z.real / s
+        out.imag = z.imag / s
+        return out
+
+    # ---- operators (tools/finite_differences.f90)
+    @staticmethod
+    def dx1(f, h):
+        res = 0.50 / h
+        df = np.empty_like(f)
+        df[0] = (-3.0 * f[0] + 4.0 * f[1] - f[2]) * res
+        df[1:-1] = (-f[:-2] + f[2:]) * res
+        df[-1] = (+3.0 * f[-1] - 4.0 * f[-2] + f[-3]) * res
+        return df
+
+    def dx2(self, f, h, inpar=False):
+        res = 0.50 / h
+        df = np.empty_like(f)
+        nz = self.kR
+        dis = nz // 2
+        df[:, 0, :] = (-3.0 * f[:, 0, :] + 4.0 * f[:, 1, :] - f[:, 2, :]) * res
+        for k in range(0, nz + 1):
+            kt = (k + dis) % (nz - 1)
+            if inpar:
+                df[:, 0, k] = (f[:, 2, kt] + f[:, 1, k]) * res
+            else:
+                df[:, 0, k] = (-f[:, 1, k] + f[:, 2, kt]) * res
+        df[:, 1:-1, :] = (-f[:, :-2, :] + f[:, 2:, :]) * res
+        df[:, -1, :] = (+3.0 * f[:, -1, :] - 4.0 * f[:, -2, :] + f[:, -3, :]) * res
+        return df
+
+    @staticmethod
+    def dx3(f, h):
+        res = 0.50 / h
+        df = np.empty_like(f)
+        nz = f.shape[2] - 1
+        df[:, :, 0] = (-f[:, :, nz - 2] + f[:, :, 1]) * res
+        df[:, :, 1:-1] = (-f[:, :, :-2] + f[:, :, 2:]) * res
+        df[:, :, nz] = (-f[:, :, 2] + f[:, :, nz - 1]) * res
+        return df
+
+    def ad1(self, f, beta, h):
+        res = 0.5 / h
+        df = np.empty_like(f)
+        n = f.shape[0] - 1
+        df[0] = (-3.0 * f[0] + 4.0 * f[1] - f[2]) * res
+        df[1] = (-3.0 * f[1] + 4.0 * f[2] - f[3]) * res
+        fw = (-3.0 * f[2:n - 1] + 4.0 * f[3:n] - f[4:n + 1]) * res
+        bw = (3.0 * f[2:n - 1] - 4.0 * f[1:n - 2] + f[0:n - 3]) * res
+        ce = (f[3:n] - f[1:n - 2]) * res
+        b = np.broadcast_to(beta[2:n - 1], fw.shape)
+        df[2:n - 1] = np.where(b > 0.0, fw, np.where(b < 0.0, bw, ce))
+        df[n - 1] = (f[n] - f[n - 2]) * res
+        df[n] = (3.0 * f[n] - 4.0 * f[n - 1] + f[n - 2]) * res
+        return df
+
+    # ---- RHS (MoL/lines_method_lib.f90:671-753)
+    def rhs_phi(self, v):
+        return self._b(self.alpha) * v[4] + self._b(self.beta[0]) * v[1]
+
+    def rhs_psi1(self, v):
+        al, b1 = self._b(self.alpha), self._b(self.beta[0])
+        return self.dx1(al * v[4], self.dx) + b1 * self.ad1(v[1], b1, self.dx) + self._b(self.dx_beta) * v[1]
+
+    def rhs_psi2(self, v):
+        return self.dx2(self._b(self.alpha) * v[4] + self._b(self.beta[0]) * v[1], self.dy, False)
+
+    def rhs_psi3(self, v):
+        return self.dx3(self._b(self.alpha) * v[4] + self._b(self.beta[0]) * v[1], self.dz)
+
+    def rhs_pi(self, v):
+        al, sg, b1 = self._b(self.alpha), self._b(self.sqrtg), self._b(self.beta[0])
+        g = lambda a, b: self._b(self.gamma_up[a, b])
+        if self.metric == "Kerr_Schild":
+            return (self.cdiv(self.dx1(al * sg * (g(0, 0) * v[1] + g(0, 2) * v[3]), self.dx), sg)
+                    + self.cdiv(self.dx2(al * sg * g(1, 1) * v[2], self.dy, False), sg)
+                    + self.cdiv(self.dx3(al * sg * (g(0, 2) * v[1] + g(2, 2) * v[3]), self.dz), sg)
+                    + v[4] * self._b(self.dx_beta)
+                    + self.cdiv(b1 * self.ad1(v[4] * sg, b1, self.dx), sg)
+                    - al * self.m ** 2 * v[0])
+        return (self.cdiv(self.dx1(al * sg * g(0, 0) * v[1], self.dx), sg)
+                + self.cdiv(self.dx2(al * sg * g(1, 1) * v[2], self.dy, False), sg)
+                + self.dx3(al * g(2, 2) * v[3], self.dz)
+                + v[4] * self._b(self.dx_beta)
+                + self.cdiv(b1 * self.ad1(v[4] * sg, b1, self.dx), sg)
+                - al * self.m ** 2 * v[0])
+
+    def rhs_all(self, v):
+        return np.stack([self.rhs_phi(v), self.rhs_psi1(v), self.rhs_psi2(v), self.rhs_psi3(v), self.rhs_pi(v)])
+
+    # ---- boundaries (MoL/lines_method_lib.f90:507-597)
+    def boundary(self):
+        u = self.u
+        u[:, 0] = 3.0 * u[:, 1] - 3.0 * u[:, 2] + u[:, 3]
+        if self.bc == "outflow":
+            u[:, -1] = u[:, -2]
+        else:
+            u[:, -1] = self.u_p[:, -1]
+        nz, ny, g = self.Nz, self.Ny, self.g
+        dis = nz // 2
+        for k in range(0, nz + 1):
+            kt = (k + dis) % (nz - 1)
+            for gg in range(g, -1, -1):
+                u[:, :, -gg - self.jL, k] = u[:, :, gg + 1 - self.jL, kt]
+        for k in range(0, nz + 1):
+            kt = (k + dis) % (nz - 1)
+            for gg in range(g, -1, -1):
+                u[:, :, ny + gg - self.jL, k] = u[:, :, ny - gg - 1 - self.jL, kt]
+        u[:, :, :, 0] = u[:, :, :, nz - 1]
+        u[:, :, :, nz] = u[:, :, :, 1]
+
+    # ---- steppers (MoL/lines_method_lib.f90:211-474)
+    def pirk2(self):
+        dt = self.dt
+        self.u_p = self.u.copy()
+        r = np.stack([self.rhs_phi(self.u), self.rhs_psi1(self.u), self.rhs_psi2(self.u), self.rhs_psi3(self.u)])
+        self.u_stage[0:4] = self.u[0:4] + dt * r
+        self.u_stage[4] = self.u[4] + dt * self.rhs_pi(self.u_stage)
+        self.boundary()
+        r = self.rhs_all(self.u_stage)
+        self.u = 0.5 * (self.u_p + self.u_stage + dt * r)
+        self.boundary()
+        self.t += dt
+
+    def pirk3(self):
+        dt = self.dt
+        self.u_p = self.u.copy()
+        r = np.stack([self.rhs_phi(self.u), self.rhs_psi1(self.u), self.rhs_psi2(self.u), self.rhs_psi3(self.u)])
+        self.u_stage[0:4] = self.u[0:4] + dt * r
+        self.u_stage[4] = self.u[4] + dt * self.rhs_pi(self.u_stage)
+        self.boundary()
+        r = np.stack([self.rhs_phi(self.u_stage), self.rhs_psi1(self.u_stage), self.rhs_psi2(self.u_stage),
+                      self.rhs_psi3(self.u_stage)])
+        self.u_stage_2[0:4] = 0.75 * self.u_p[0:4] + 0.25 * (self.u_stage[0:4] + dt * r)
+        self.u_stage_2[4] = 0.75 * self.u_p[4] + 0.25 * (self.u_stage[4] + dt * self.rhs_pi(self.u_stage_2))
+        self.boundary()
+        r = self.rhs_all(self.u_stage_2)
+        self.u = (1.0 / 3.0) * self.u_p + (2.0 / 3.0) * (self.u_stage_2 + dt * r)
+        self.boundary()
+        self.t += dt
+
+    def rk3(self):
+        dt = self.dt
+        self.u_p = self.u.copy()
+        for rk in (1, 2, 3):
+            r = self.rhs_all(self.u)
+            if rk == 1:
+                self.u = self.u_p + r * dt
+            elif rk == 2:
+                self.u = 0.750 * self.u_p + 0.250 * (self.u + r * dt)
+            else:
+                self.u = self.cdiv(self.u_p, 3.0) + self.cdiv(2.0 * (self.u + r * dt), 3.0)
+            self.boundary()
+        self.t += dt
+
+    def rk4(self):
+        dt = self.dt
+        self.u_p = self.u.copy()
+        ks = []
+        for rk in (1, 2, 3, 4):
+            r = self.rhs_all(self.u)
+            kk = r * dt
+            ks.append(kk)
+            if rk in (1, 2):
+                self.u = self.u_p + 0.50 * kk
+            elif rk == 3:
+                self.u = self.u_p + kk
+            else:
+                self.u = self.u_p + self.cdiv(ks[0] + 2.0 * ks[1] + 2.0 * ks[2] + ks[3], 6.0)
+            self.boundary()
+        self.t += dt
+
+    # ---- Fortran-order state helpers: u(5, NI, NJ, NK) complex, var fastest
+    def set_state(self, fortran_u):
+        self.u = np.ascontiguousarray(np.asarray(fortran_u).reshape(self.NK, self.NJ, self.NI, 5).transpose(3, 2, 1, 0))
+
+    def get_state(self):
+        return np.ascontiguousarray(self.u.transpose(3, 2, 1, 0)).reshape(-1)
