@@ -136,7 +136,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(w, threads, nx_sample=64, steps=2):
+def cpu_baseline(w, threads, nx_sample=128, steps=60):
     """The oracle (CPU restatement of the reference path) on a radial slab of the
     workload: same theta x phi grid, Nx = nx_sample cells, `steps` PIRK2 steps."""
     from oracle.oracle import Oracle, set_threads
@@ -164,7 +164,7 @@ def run_reference(args):
     from oracle.oracle import Oracle, set_threads
     from kg_b200.initial_data import shell_ylm
     set_threads(threads)
-    Nx = 64
+    Nx = 128
     xmax = w["xmin"] + (w["xmax"] - w["xmin"]) * Nx / w["Nx"]
     o = Oracle(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, CFL=w["CFL"], m=w["m"])
     u0, _ = shell_ylm(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, seed=w["seed"], r0=8.0)
@@ -195,7 +195,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kg", choices=["kg", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", default=None,
+                    help="Nx,Ny,Nz override (profiling captures of a smaller case); r range scales with Nx")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and other-stepper legs")
     args = ap.parse_args()
+    if args.grid:
+        nx, ny, nz = (int(v) for v in args.grid.split(","))
+        WORKLOAD.update(Nx=nx, Ny=ny, Nz=nz,
+                        xmax=WORKLOAD["xmin"] + (WORKLOAD["xmax"] - WORKLOAD["xmin"]) * nx / 2048)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -261,7 +268,7 @@ def main():
     # other steppers, briefly (device-resident, same grid)
     per_stepper = {}
     stages = {"pirk2": 2, "pirk3": 3, "rk3": 3, "rk4": 4}
-    for meth in ("pirk3", "rk3", "rk4"):
+    for meth in (() if args.no_e2e else ("pirk3", "rk3", "rk4")):
         getattr(mol, meth)(nsteps=1) if meth.startswith("rk") else getattr(mol, meth)(1)
         mol.synchronize()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -287,11 +294,12 @@ def main():
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
-    mol._ck(lib.kg_set_state(h, 0, p_in))
-    for l in range(1, args.steps + 1):
-        mol._ck(lib.kg_pirk2(h, 1))
-        mol._ck(lib.kg_diagnostic(h, l, C.byref(mass)))
-    mol._ck(lib.kg_get_state(h, 0, p_out))
+    if not args.no_e2e:
+        mol._ck(lib.kg_set_state(h, 0, p_in))
+        for l in range(1, args.steps + 1):
+            mol._ck(lib.kg_pirk2(h, 1))
+            mol._ck(lib.kg_diagnostic(h, l, C.byref(mass)))
+        mol._ck(lib.kg_get_state(h, 0, p_out))
     f1.record(stream)
     f1.synchronize()
     t = torch.tensor([f0.elapsed_time(f1)], device=f"cuda:{local}", dtype=torch.float64)
@@ -304,7 +312,8 @@ def main():
     e2e_value = world * pts * 2 * args.steps / (e2e_ms / 1e3)
 
     # roofline of the dominant kernel
-    dom = max(kinds.items(), key=lambda kv: kv[1][0])[0] if kinds else "stage_pirk2_s2"
+    stage_kinds = {k: v for k, v in kinds.items() if k in ALG_BYTES}
+    dom = max(stage_kinds.items(), key=lambda kv: kv[1][0])[0] if stage_kinds else "stage_pirk2_s2"
     dms, dcnt = kinds.get(dom, (0.0, 1))
     peak, peak_kind = measured_peaks()
     alg = ALG_BYTES.get(dom, 0) * stored_points(w)
@@ -322,8 +331,9 @@ def main():
             "step_bandwidth_gbs": step_bytes / (el_ms / args.steps / 1e3) / 1e9,
             "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in kinds.items()},
             "steppers_gpsu": dict(per_stepper, pirk2=value / world),
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
-                    "d2h_bytes_per_step": (state_bytes + 8 * args.steps) / args.steps},
+            "e2e": None if args.no_e2e else {
+                "value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
+                "d2h_bytes_per_step": (state_bytes + 8 * args.steps) / args.steps},
             "gpu_launches": int(launches), "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -78,6 +78,7 @@ SIGNATURES = [
     ("kg_profile_kinds", _I, []),
     ("kg_profile_kind_name", C.c_char_p, [_I]),
     ("kg_launch_count", C.c_longlong, [_P]),
+    ("kg_set_kernel_variant", _I, [_P, _I]),
 ]
 
 _lib = None

@@ -26,7 +26,7 @@ using kg::Metric;
 namespace {
 
 enum { T_ALPHA = 0, T_BETA, T_DXBETA, T_SQRTG, T_ASG, T_GRR, T_GRP, T_GPP, T_ASG_GTT, T_ASG_GRR, T_A_GPP, T_AM2,
-       T_GTT, T_COUNT };
+       T_GTT, T_RSG, T_COUNT };
 
 }  // namespace
 
@@ -58,6 +58,7 @@ struct kg_solver {
   double* rho = nullptr;
   double* partials = nullptr;            // mass partial sums + result
   int s_cur = 4, t_cur = 4;              // slot holding the current Pi stage value
+  int variant = 1;                       // 0: per-point kernels, 1: 2.5-D marching kernels
   // detectors and projection
   int n_det = 5;
   std::vector<double> r_det;
@@ -308,6 +309,7 @@ void derive_tables(kg_solver* h) {
     TB(T_ASG_GRR, q) = asg * TB(T_GRR, q);
     TB(T_A_GPP, q) = TB(T_ALPHA, q) * TB(T_GPP, q);
     TB(T_AM2, q) = TB(T_ALPHA, q) * m2;
+    TB(T_RSG, q) = 1.0 / TB(T_SQRTG, q);  // correctly rounded reciprocal for the Markstein quotient
   }
 }
 
@@ -594,7 +596,10 @@ int store_view(kg_solver* h, const View& V, double* dst, cudaMemcpyKind kind) {
 
 void run_stage(kg_solver* h, int kind, const kg::StageLaunch& L) {
   Prof pf(h, kind, 1);
-  kg::launch_stage(kind, L, h->stream);
+  if (h->variant == 1)
+    kg::launch_stage_march(kind, L, h->dmet + (size_t)T_RSG * h->NJ * h->PI, h->stream);
+  else
+    kg::launch_stage(kind, L, h->stream);
 }
 void run_ghost(kg_solver* h, double2* u, const double2* up, int inflow) {
   Prof pf(h, PK_GHOST, 2);
@@ -1110,6 +1115,12 @@ int kg_sph_harmonics(kg_solver* h, int L, double* out) {
           }
         }
       }
+  return KG_OK;
+}
+
+int kg_set_kernel_variant(kg_solver* h, int variant) {
+  if (!h || variant < 0 || variant > 1) return KG_EINVAL;
+  h->variant = variant;
   return KG_OK;
 }
 

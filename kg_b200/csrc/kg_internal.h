@@ -37,6 +37,8 @@ struct StageLaunch {
 };
 
 void launch_stage(int kind, const StageLaunch& L, cudaStream_t st);
+// 2.5-D marching form of the same kernels (kg_march.cu); rsg = 1/sqrt(gamma) table
+void launch_stage_march(int kind, const StageLaunch& L, const double* rsg, cudaStream_t st);
 void launch_rhs(const Grid& g, const Metric& m, int metric_kind, const double2* const in[5], double2* out,
                 unsigned mask, cudaStream_t st);
 
