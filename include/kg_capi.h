@@ -71,6 +71,8 @@ typedef struct kg_solver kg_solver;
 int kg_create(const kg_params *p, int device, kg_solver **out);
 /* no reference counterpart (the reference never deallocates) */
 int kg_destroy(kg_solver *h);
+/* text of the handle's last error; with h = NULL, of the calling thread's
+ * last handle-less call */
 const char *kg_last_error(const kg_solver *h);
 /* scalars: dx, dy, dz, dt, t, xmin, xmax, Nt, r_max (9 doubles) */
 int kg_get_scalars(const kg_solver *h, double *out9);
@@ -168,6 +170,27 @@ long long kg_launch_count(const kg_solver *h);
 /* stage-kernel form: 1 = 2.5-D marching kernels (default), 0 = one thread per
  * point with cached neighbour loads; both give bit-identical results */
 int kg_set_kernel_variant(kg_solver *h, int variant);
+
+/* --- allocation-free diagnostic --------------------------------------------- */
+
+/* Mass_scalar = integrate(rho*sqrtg) without allocating anything.  No
+ * counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc -- a host that records its time loop into a CUDA graph (an
+ * allocation inside a stream capture breaks the capture) or whose device
+ * memory belongs to its own pool or a fixed budget already given to live
+ * solves.  The caller passes everything in its own device memory: rho as
+ * (Nz+1) x (Ny+2g+1) x (Nx+2g+1) doubles (r fastest, ghosts included, g = 2),
+ * sqrtg as (Ny+2g+1) x (Nx+2g+1), and one double for the result; the work is
+ * enqueued on `stream` (a cudaStream_t, NULL for the default stream) and the
+ * call returns without waiting.  Intermediate sums live in a static device
+ * array of 2^19 doubles (4 MiB, held by every GPU that loads the library
+ * until exit): a grid needing more than (Nx+1)*(Ny+1) + Nx+1 <= 2^19 is
+ * rejected with KG_EINVAL, text in kg_last_error(NULL).  Calls share that
+ * array, so calls that overlap on the GPU race.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress, with that device
+ * current) and must come before any stream capture. */
+int kg_integrate_mass_noalloc(const double *rho_dev, const double *sqrtg_dev, int Nx, int Ny, int Nz,
+                              double dx, double dy, double dz, double *out_dev, void *stream);
 
 #ifdef __cplusplus
 }

@@ -79,6 +79,8 @@ SIGNATURES = [
     ("kg_profile_kind_name", C.c_char_p, [_I]),
     ("kg_launch_count", C.c_longlong, [_P]),
     ("kg_set_kernel_variant", _I, [_P, _I]),
+    ("kg_integrate_mass_noalloc", _I, [C.c_void_p, C.c_void_p, _I, _I, _I, C.c_double, C.c_double,
+                                       C.c_double, C.c_void_p, C.c_void_p]),
 ]
 
 _lib = None

@@ -23,6 +23,8 @@
 using kg::Grid;
 using kg::Metric;
 
+const char* kg_noalloc_last_error();  // kg_noalloc.cu
+
 namespace {
 
 enum { T_ALPHA = 0, T_BETA, T_DXBETA, T_SQRTG, T_ASG, T_GRR, T_GRP, T_GPP, T_ASG_GTT, T_ASG_GRR, T_A_GPP, T_AM2,
@@ -697,7 +699,7 @@ int kg_destroy(kg_solver* h) {
   return KG_OK;
 }
 
-const char* kg_last_error(const kg_solver* h) { return h ? h->err.c_str() : "null handle"; }
+const char* kg_last_error(const kg_solver* h) { return h ? h->err.c_str() : kg_noalloc_last_error(); }
 
 int kg_get_scalars(const kg_solver* h, double* o) {
   if (!h || !o) return KG_EINVAL;
