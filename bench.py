@@ -198,6 +198,7 @@ def main():
     ap.add_argument("--grid", default=None,
                     help="Nx,Ny,Nz override (profiling captures of a smaller case); r range scales with Nx")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and other-stepper legs")
+    ap.add_argument("--variant", type=int, default=None, help="stage-kernel form (kg_set_kernel_variant)")
     args = ap.parse_args()
     if args.grid:
         nx, ny, nz = (int(v) for v in args.grid.split(","))
@@ -224,6 +225,8 @@ def main():
     mol = ScalarField(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], m=w["m"], device=local,
                       save=10 * 0.25 * 0.0018, l_max=8)
     lib, h = mol._lib, mol.handle
+    if args.variant is not None:
+        mol._ck(lib.kg_set_kernel_variant(h, args.variant))
     u0, _ = shell_ylm_device(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], seed=w["seed"] + rank,
                              device=f"cuda:{local}")
     mol._ck(lib.kg_set_state_device(h, 0, C.c_void_p(u0.data_ptr())))

@@ -167,8 +167,9 @@ int kg_profile_kinds(void);
 const char *kg_profile_kind_name(int kind);
 /* total kernel launches issued by the handle since creation */
 long long kg_launch_count(const kg_solver *h);
-/* stage-kernel form: 1 = 2.5-D marching kernels (default), 0 = one thread per
- * point with cached neighbour loads; both give bit-identical results */
+/* stage-kernel form: 2 = marching kernels fed by a TMA shared-memory ring
+ * (default), 1 = 2.5-D marching kernels with register prefetch, 0 = one thread
+ * per point with cached neighbour loads; all give bit-identical results */
 int kg_set_kernel_variant(kg_solver *h, int variant);
 
 /* --- allocation-free diagnostic --------------------------------------------- */

@@ -60,7 +60,8 @@ struct kg_solver {
   double* rho = nullptr;
   double* partials = nullptr;            // mass partial sums + result
   int s_cur = 4, t_cur = 4;              // slot holding the current Pi stage value
-  int variant = 1;                       // 0: per-point kernels, 1: 2.5-D marching kernels
+  int variant = 2;                       // 0: per-point, 1: 2.5-D marching, 2: TMA-pipelined marching
+  int* derr = nullptr;                   // device flag: a bounded wait in a kernel ran out
   // detectors and projection
   int n_det = 5;
   std::vector<double> r_det;
@@ -598,10 +599,24 @@ int store_view(kg_solver* h, const View& V, double* dst, cudaMemcpyKind kind) {
 
 void run_stage(kg_solver* h, int kind, const kg::StageLaunch& L) {
   Prof pf(h, kind, 1);
-  if (h->variant == 1)
-    kg::launch_stage_march(kind, L, h->dmet + (size_t)T_RSG * h->NJ * h->PI, h->stream);
+  const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
+  if (h->variant == 2 && kg::launch_stage_tma(kind, L, rsg, h->derr, h->stream) == 0) return;
+  if (h->variant >= 1)
+    kg::launch_stage_march(kind, L, rsg, h->stream);
   else
     kg::launch_stage(kind, L, h->stream);
+}
+
+// KG_ETIMEOUT if a kernel reported a bounded wait that ran out (flag is sticky)
+int check_device_flag(kg_solver* h) {
+  int f = 0;
+  KG_CK(cudaMemcpyAsync(&f, h->derr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  if (f) {
+    h->err = "a device wait ran out (TMA stage kernel); results of the affected launch are invalid";
+    return KG_ETIMEOUT;
+  }
+  return KG_OK;
 }
 void run_ghost(kg_solver* h, double2* u, const double2* up, int inflow) {
   Prof pf(h, PK_GHOST, 2);
@@ -670,6 +685,7 @@ int kg_create(const kg_params* p, int device, kg_solver** out) {
   if ((rc = dalloc(h, (void**)&h->dmet, (size_t)T_COUNT * h->NJ * h->PI * sizeof(double))) ||
       (rc = upload_tables(h)) || (rc = dalloc(h, (void**)&h->U, 5 * field_bytes(h))) ||
       (rc = dalloc(h, (void**)&h->partials, (size_t)(kg::mass_blocks(g) + 1) * sizeof(double))) ||
+      (rc = dalloc(h, (void**)&h->derr, 16)) ||
       (rc = build_detectors(h))) {
     kg_destroy(h);
     return rc;
@@ -678,6 +694,7 @@ int kg_create(const kg_params* p, int device, kg_solver** out) {
     kg_destroy(h);
     return KG_ECUDA;
   }
+  if (!kg::tma_available(h->g, h->U)) h->variant = 1;  // tensor maps unavailable: register-prefetch form
   *out = h;
   return KG_OK;
 }
@@ -686,7 +703,7 @@ int kg_destroy(kg_solver* h) {
   if (!h) return KG_EINVAL;
   if (h->stream) cudaStreamSynchronize(h->stream);
   void* bufs[] = {h->dmet, h->U, h->S, h->T, h->RK, h->UP, h->HV, h->stage_buf, h->rho, h->partials,
-                  h->d_int, h->d_dbl, h->shells, h->alm, h->flux};
+                  h->d_int, h->d_dbl, h->shells, h->alm, h->flux, h->derr};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (auto& r : h->recs) {
@@ -727,7 +744,7 @@ size_t kg_device_bytes(const kg_solver* h) { return h ? h->bytes : 0; }
 int kg_synchronize(kg_solver* h) {
   if (!h) return KG_EINVAL;
   KG_CK(cudaStreamSynchronize(h->stream));
-  return KG_OK;
+  return check_device_flag(h);
 }
 
 int kg_set_state(kg_solver* h, int which, const double* host_u) {
@@ -747,7 +764,7 @@ int kg_get_state(kg_solver* h, int which, double* host_u) {
   if ((rc = state_view(h, which, &V))) return rc;
   if ((rc = store_view(h, V, host_u, cudaMemcpyDeviceToHost))) return rc;
   KG_CK(cudaStreamSynchronize(h->stream));
-  return KG_OK;
+  return check_device_flag(h);
 }
 
 int kg_set_state_device(kg_solver* h, int which, const double* dev_u) {
@@ -1121,7 +1138,7 @@ int kg_sph_harmonics(kg_solver* h, int L, double* out) {
 }
 
 int kg_set_kernel_variant(kg_solver* h, int variant) {
-  if (!h || variant < 0 || variant > 1) return KG_EINVAL;
+  if (!h || variant < 0 || variant > 2) return KG_EINVAL;
   h->variant = variant;
   return KG_OK;
 }

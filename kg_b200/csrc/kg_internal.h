@@ -39,6 +39,11 @@ struct StageLaunch {
 void launch_stage(int kind, const StageLaunch& L, cudaStream_t st);
 // 2.5-D marching form of the same kernels (kg_march.cu); rsg = 1/sqrt(gamma) table
 void launch_stage_march(int kind, const StageLaunch& L, const double* rsg, cudaStream_t st);
+// TMA-pipelined form (kg_tma.cu); err: device flag set to 1 when a bounded wait runs out.
+// Returns 0, or -1 if the tensor maps cannot be encoded / the kernel cannot be configured.
+int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st);
+// true when the driver can encode the tensor maps the TMA form needs for this grid
+bool tma_available(const Grid& g, const double2* some_state);
 void launch_rhs(const Grid& g, const Metric& m, int metric_kind, const double2* const in[5], double2* out,
                 unsigned mask, cudaStream_t st);
 

@@ -1,0 +1,485 @@
+// kg_tma.cu -- TMA-pipelined form of the fused RHS + stage kernels.
+//
+// Same arithmetic as kg_stencil.cu and kg_march.cu, bit for bit; the memory
+// side is organised for Blackwell:
+//   * a CTA owns a 32 x 8 tile of (r, theta) columns and marches through a
+//     chunk of phi planes;
+//   * every plane the CTA needs -- the tile with a +-2 r halo and a +-1 theta
+//     halo, all five stencil inputs -- is brought into a 3-deep shared-memory
+//     ring by the tensor-memory accelerator (cp.async.bulk.tensor, two boxes
+//     per plane: variables 1-4 and the Pi variable, which the PIRK stages keep
+//     in a separate slot), completion tracked by one mbarrier per ring slot;
+//     while the CTA computes plane k, the loads of planes k+1 and k+2 are in
+//     flight, so HBM latency is hidden without holding prefetched values in
+//     registers;
+//   * the phi-derivative arguments of the thread's own column roll in
+//     registers; r and theta neighbours are read from the ring and combined
+//     with a per-CTA metric tile that is loaded once (the metric is
+//     phi-independent);
+//   * divisions by sqrt(gamma) use the correctly rounded host reciprocal and
+//     one Markstein step (see kg_march.cu), equal to IEEE division.
+// All TMA coordinates are multiples of 16 bytes in x (the r axis is addressed
+// in doubles, two per complex value) and the boxes start at most 2 points
+// before the array or one row above it, where the loads read zeros.  Waits on
+// the mbarriers are bounded: a CTA that runs out sets the error flag, waits
+// (bounded) for its own copies and returns; the host reports KG_ETIMEOUT.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include "kg_device.cuh"
+#include "kg_internal.h"
+
+namespace kg {
+namespace {
+
+constexpr int TI = 32, TJ = 8, RH = 2;
+constexpr int RW = 2 * (TI + 2 * RH);         // ring row width in doubles (72 = 576 B)
+constexpr int RROWS = TJ + 2;                 // theta rows with halo
+constexpr int FIELD_D = RROWS * RW;           // doubles per variable per plane
+constexpr int STAGE_D = 5 * FIELD_D;          // doubles per ring slot
+constexpr int STAGE_B = STAGE_D * 8;          // 28800 bytes
+constexpr int NST = 3;                        // ring depth
+constexpr int MW = TI + 2 * RH, MH = TJ + 2;  // metric tile
+constexpr int MT_N = MW * MH;
+enum { MT_AL = 0, MT_BE, MT_A, MT_GRR, MT_GRP, MT_SG, MT_HT, MT_COUNT };
+constexpr size_t SMEM_BYTES = (size_t)NST * STAGE_B + (size_t)MT_COUNT * MT_N * 8 + 64;
+constexpr long long WAIT_LIMIT = 1LL << 24;
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(saddr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity) {
+  for (long long it = 0; it < WAIT_LIMIT; ++it)
+    if (mbar_try_wait(b, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(saddr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(saddr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ double ddiv(double a, double b, double rb) {
+  const double q = a * rb;
+  const double r = __fma_rn(-q, b, a);
+  return __fma_rn(r, rb, q);
+}
+__device__ __forceinline__ double2 cdivm(double2 a, double b, double rb) {
+  return c2(ddiv(a.x, b, rb), ddiv(a.y, b, rb));
+}
+
+struct TmaArgs {
+  Grid g;
+  Metric m;
+  const double* rsg;
+  const double2* in[5];  // for direct (out-of-tile) reads
+  const double2* base;
+  const double2* aux4;
+  double2* out;
+  double2* out4;
+  double2* acc;
+  int skip_last_i;
+  int kchunk;
+  int* err;
+};
+
+}  // namespace
+
+template <int KIND, int MK>
+__global__ void __launch_bounds__(TI * TJ, 2)
+    tma_stage_kernel(const __grid_constant__ CUtensorMap tm4, const __grid_constant__ CUtensorMap tm1, TmaArgs a) {
+  constexpr bool PSI = (KIND != ST_P2_S1B && KIND != ST_P3_S2B);
+  constexpr bool PI_ = (KIND != ST_P2_S1A && KIND != ST_P3_S2A);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  double* ring = reinterpret_cast<double*>(smem_raw);
+  double* mt = ring + (size_t)NST * STAGE_D;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
+
+  const Grid& g = a.g;
+  const Metric& M = a.m;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TI + tx;
+  const int ii0 = blockIdx.x * TI, jj0 = blockIdx.y * TJ;
+  const int ii = ii0 + tx, jj = jj0 + ty;
+  const bool act = (ii < g.NI) && (jj < g.NJ);
+  const int k0 = blockIdx.z * a.kchunk;
+  if (k0 >= g.NK) return;
+  const int k1 = min(k0 + a.kchunk, g.NK);
+  const int nplanes = (k1 - k0) + 2;  // previous, the chunk, next
+  auto plane_of = [&](int t) -> int {
+    if (t == 0) return (k0 == 0) ? g.Nz - 2 : k0 - 1;
+    if (t <= k1 - k0) return k0 + t - 1;
+    return (k1 - 1 == g.Nz) ? 2 : k1;
+  };
+  auto issue = [&](int t) {
+    const int s = t % NST;
+    uint64_t* b = &bars[s];
+    double* dst = ring + (size_t)s * STAGE_D;
+    mbar_expect_tx(b, STAGE_B);
+    const int z = plane_of(t);
+    tma_load_4d(dst, &tm4, 2 * (ii0 - RH), jj0 - 1, z, 0, b);
+    tma_load_4d(dst + 4 * FIELD_D, &tm1, 2 * (ii0 - RH), jj0 - 1, z, 0, b);
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // metric tile (phi-independent), zero outside the array
+  for (int t = tid; t < MT_N; t += TI * TJ) {
+    const int mx = t % MW, my = t / MW;
+    const int gi = ii0 - RH + mx, gj = jj0 - 1 + my;
+    const bool in = gi >= 0 && gi < g.NI && gj >= 0 && gj < g.NJ;
+    const int q = in ? off2(g, gi, gj) : 0;
+    mt[MT_AL * MT_N + t] = in ? ldm(M.alpha, q) : 0.0;
+    mt[MT_BE * MT_N + t] = in ? ldm(M.beta, q) : 0.0;
+    mt[MT_A * MT_N + t] = in ? ldm(MK == MK_KS ? M.asg : M.asg_grr, q) : 0.0;
+    mt[MT_GRR * MT_N + t] = in ? ldm(M.grr, q) : 0.0;
+    mt[MT_GRP * MT_N + t] = in ? ldm(M.grp, q) : 0.0;
+    mt[MT_SG * MT_N + t] = in ? ldm(M.sqrtg, q) : 0.0;
+    mt[MT_HT * MT_N + t] = in ? ldm(M.asg_gtt, q) : 0.0;
+  }
+  __syncthreads();
+  int nissued = 0;  // meaningful in thread 0 only
+  if (tid == 0)
+    for (int t = 0; t < NST && t < nplanes; ++t) {
+      issue(t);
+      nissued = t + 1;
+    }
+
+  // own-point metric
+  const int q = act ? off2(g, ii, jj) : 0;
+  double al = 0, be = 0, dxb = 0, sg = 1, rs = 1, am2 = 0, fa = 0, fgrp = 0, fgpp = 0;
+  if (act) {
+    al = ldm(M.alpha, q);
+    be = ldm(M.beta, q);
+    dxb = ldm(M.dxbeta, q);
+    sg = ldm(M.sqrtg, q);
+    rs = ldm(a.rsg, q);
+    am2 = ldm(M.am2, q);
+    if (MK == MK_KS) {
+      fa = ldm(M.asg, q);
+      fgrp = ldm(M.grp, q);
+      fgpp = ldm(M.gpp, q);
+    } else {
+      fa = ldm(M.a_gpp, q);
+    }
+  }
+  const long long pcol = act ? off3(g, ii, jj, 0) : 0;
+  auto RF = [&](const double* st, int f, int dx, int dy) -> double2 {
+    return *reinterpret_cast<const double2*>(st + (size_t)f * FIELD_D + (dy + 1) * RW + 2 * (dx + RH));
+  };
+  auto MTV = [&](int which, int dx, int dy) -> double { return mt[which * MT_N + (dy + 1) * MW + dx + RH]; };
+  auto phiE = [&](const double* st) { return cadd(rmul(al, RF(st, 4, tx, ty)), rmul(be, RF(st, 1, tx, ty))); };
+  auto phiF = [&](const double* st) {
+    if (MK == MK_KS) return rmul(fa, cadd(rmul(fgrp, RF(st, 1, tx, ty)), rmul(fgpp, RF(st, 3, tx, ty))));
+    return rmul(fa, RF(st, 3, tx, ty));
+  };
+
+  int timed_out = 0;
+  double2 Epv = c2(0, 0), Fpv = c2(0, 0), Ecu = c2(0, 0), Fcu = c2(0, 0);
+  if (!mbar_wait_bounded(&bars[0], 0)) timed_out = 1;
+  if (act && !timed_out) {
+    const double* st = ring;
+    if (PSI) Epv = phiE(st);
+    if (PI_) Fpv = phiF(st);
+  }
+  bool failed = __syncthreads_or(timed_out) != 0;
+
+  for (int i = 0; i < k1 - k0 && !failed; ++i) {
+    const int k = k0 + i;
+    if (tid == 0 && i + NST < nplanes) {
+      issue(i + NST);
+      nissued = i + NST + 1;
+    }
+    {
+      const int tc = i + 1, tn = i + 2;
+      const bool okc = mbar_wait_bounded(&bars[tc % NST], (tc / NST) & 1);
+      const bool okn = okc && mbar_wait_bounded(&bars[tn % NST], (tn / NST) & 1);
+      if (!okn) timed_out = 1;
+      if (act && !timed_out) {
+        const double* cu = ring + (size_t)(tc % NST) * STAGE_D;
+        const double* nx = ring + (size_t)(tn % NST) * STAGE_D;
+        if (i == 0) {
+          if (PSI) Ecu = phiE(cu);
+          if (PI_) Fcu = phiF(cu);
+        }
+        double2 Enx = c2(0, 0), Fnx = c2(0, 0);
+        if (PSI) Enx = phiE(nx);
+        if (PI_) Fnx = phiF(nx);
+        double2 fcu[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) fcu[v] = RF(cu, v, tx, ty);
+        const long long p = pcol + (long long)k * g.plane;
+        const int n = g.NI - 1;
+        double2 r[5];
+        if (PSI) {
+          r[0] = cadd(rmul(al, fcu[4]), rmul(be, fcu[1]));
+          auto aPi = [&](int dx) { return rmul(MTV(MT_AL, tx + dx, ty), RF(cu, 4, tx + dx, ty)); };
+          auto ps1 = [&](int dx) { return RF(cu, 1, tx + dx, ty); };
+          double2 d;
+          if (ii == 0) d = fwd3(aPi(0), aPi(1), aPi(2));
+          else if (ii == n) d = bwd3(aPi(0), aPi(-1), aPi(-2));
+          else d = ctr(aPi(-1), aPi(1));
+          d = rmul(g.rdx, d);
+          double2 av;
+          if (ii <= 1) av = fwd3(fcu[1], ps1(1), ps1(2));
+          else if (ii == n - 1) av = csub(ps1(1), ps1(-1));
+          else if (ii == n) av = bwd3(fcu[1], ps1(-1), ps1(-2));
+          else if (be > 0.0) av = fwd3(fcu[1], ps1(1), ps1(2));
+          else if (be < 0.0) av = bwd3(fcu[1], ps1(-1), ps1(-2));
+          else av = csub(ps1(1), ps1(-1));
+          av = rmul(g.rdx, av);
+          r[1] = cadd(cadd(d, rmul(be, av)), rmul(dxb, fcu[1]));
+          auto E = [&](int dy) {
+            return cadd(rmul(MTV(MT_AL, tx, ty + dy), RF(cu, 4, tx, ty + dy)),
+                        rmul(MTV(MT_BE, tx, ty + dy), RF(cu, 1, tx, ty + dy)));
+          };
+          auto Eg = [&](int j2, int k2) {
+            const int q2 = off2(g, ii, j2);
+            const long long p2 = off3(g, ii, j2, k2);
+            return cadd(rmul(ldm(M.alpha, q2), ldf(a.in[4], p2)), rmul(ldm(M.beta, q2), ldf(a.in[1], p2)));
+          };
+          double2 t;
+          if (jj == 0) t = cadd(cneg(E(1)), Eg(2, ktarget(g, k)));
+          else if (jj == g.NJ - 1) t = bwd3(E(0), E(-1), (ty >= 1) ? E(-2) : Eg(jj - 2, k));
+          else t = ctr(E(-1), E(1));
+          r[2] = rmul(g.rdy, t);
+          double2 z;
+          if (k == 0) z = cadd(cneg(Epv), Enx);
+          else if (k == g.Nz) z = cadd(cneg(Enx), Epv);
+          else z = ctr(Epv, Enx);
+          r[3] = rmul(g.rdz, z);
+        }
+        if (PI_) {
+          auto G1 = [&](int dx) {
+            if (MK == MK_KS)
+              return rmul(MTV(MT_A, tx + dx, ty), cadd(rmul(MTV(MT_GRR, tx + dx, ty), RF(cu, 1, tx + dx, ty)),
+                                                       rmul(MTV(MT_GRP, tx + dx, ty), RF(cu, 3, tx + dx, ty))));
+            return rmul(MTV(MT_A, tx + dx, ty), RF(cu, 1, tx + dx, ty));
+          };
+          double2 d;
+          if (ii == 0) d = fwd3(G1(0), G1(1), G1(2));
+          else if (ii == n) d = bwd3(G1(0), G1(-1), G1(-2));
+          else d = ctr(G1(-1), G1(1));
+          const double2 r1 = cdivm(rmul(g.rdx, d), sg, rs);
+          auto H = [&](int dy) { return rmul(MTV(MT_HT, tx, ty + dy), RF(cu, 2, tx, ty + dy)); };
+          auto Hg = [&](int j2, int k2) {
+            return rmul(ldm(M.asg_gtt, off2(g, ii, j2)), ldf(a.in[2], off3(g, ii, j2, k2)));
+          };
+          double2 t;
+          if (jj == 0) t = cadd(cneg(H(1)), Hg(2, ktarget(g, k)));
+          else if (jj == g.NJ - 1) t = bwd3(H(0), H(-1), (ty >= 1) ? H(-2) : Hg(jj - 2, k));
+          else t = ctr(H(-1), H(1));
+          const double2 r2 = cdivm(rmul(g.rdy, t), sg, rs);
+          double2 z;
+          if (k == 0) z = cadd(cneg(Fpv), Fnx);
+          else if (k == g.Nz) z = cadd(cneg(Fnx), Fpv);
+          else z = ctr(Fpv, Fnx);
+          z = rmul(g.rdz, z);
+          const double2 r3 = (MK == MK_KS) ? cdivm(z, sg, rs) : z;
+          const double2 r4 = rmul(dxb, fcu[4]);
+          auto Q = [&](int dx) { return rmul(MTV(MT_SG, tx + dx, ty), RF(cu, 4, tx + dx, ty)); };
+          double2 av;
+          if (ii <= 1) av = fwd3(Q(0), Q(1), Q(2));
+          else if (ii == n - 1) av = csub(Q(1), Q(-1));
+          else if (ii == n) av = bwd3(Q(0), Q(-1), Q(-2));
+          else if (be > 0.0) av = fwd3(Q(0), Q(1), Q(2));
+          else if (be < 0.0) av = bwd3(Q(0), Q(-1), Q(-2));
+          else av = csub(Q(1), Q(-1));
+          av = rmul(g.rdx, av);
+          const double2 r5 = cdivm(rmul(be, av), sg, rs);
+          const double2 r6 = rmul(am2, fcu[0]);
+          r[4] = csub(cadd(cadd(cadd(cadd(r1, r2), r3), r4), r5), r6);
+        }
+        const double dt = g.dt;
+        if (KIND == ST_P2_S1A) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v) a.out[v * g.fs + p] = cadd(ldf(a.base + v * g.fs, p), rmul(dt, r[v]));
+        } else if (KIND == ST_P3_S2A) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+            a.out[v * g.fs + p] =
+                cadd(rmul(0.75, ldf(a.base + v * g.fs, p)), rmul(0.25, cadd(fcu[v], rmul(dt, r[v]))));
+        } else if (KIND == ST_P2_S1B) {
+          a.out4[p] = cadd(ldf(a.base + 4 * g.fs, p), rmul(dt, r[4]));
+        } else if (KIND == ST_P3_S2B) {
+          a.out4[p] = cadd(rmul(0.75, ldf(a.base + 4 * g.fs, p)), rmul(0.25, cadd(ldf(a.aux4, p), rmul(dt, r[4]))));
+        } else if (!(a.skip_last_i && ii == n)) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) {
+            const long long o = v * g.fs + p;
+            const double2 b = ldf(a.base + v * g.fs, p);
+            double2 res;
+            if (KIND == ST_P2_S2) {
+              res = rmul(0.5, cadd(cadd(b, fcu[v]), rmul(dt, r[v])));
+            } else if (KIND == ST_P3_S3) {
+              res = cadd(rmul(1.0 / 3.0, b), rmul(2.0 / 3.0, cadd(fcu[v], rmul(dt, r[v]))));
+            } else if (KIND == ST_RK3_1) {
+              res = cadd(b, rmul(dt, r[v]));
+            } else if (KIND == ST_RK3_2) {
+              res = cadd(rmul(0.750, b), rmul(0.250, cadd(fcu[v], rmul(dt, r[v]))));
+            } else if (KIND == ST_RK3_3) {
+              res = cadd(cdivr(b, 3.0), cdivr(rmul(2.0, cadd(fcu[v], rmul(dt, r[v]))), 3.0));
+            } else if (KIND == ST_RK4_1) {
+              const double2 kk = rmul(dt, r[v]);
+              a.acc[o] = kk;
+              res = cadd(b, rmul(0.50, kk));
+            } else if (KIND == ST_RK4_2) {
+              const double2 kk = rmul(dt, r[v]);
+              a.acc[o] = cadd(a.acc[o], rmul(2.0, kk));
+              res = cadd(b, rmul(0.50, kk));
+            } else if (KIND == ST_RK4_3) {
+              const double2 kk = rmul(dt, r[v]);
+              a.acc[o] = cadd(a.acc[o], rmul(2.0, kk));
+              res = cadd(b, kk);
+            } else {
+              const double2 kk = rmul(dt, r[v]);
+              res = cadd(b, cdivr(cadd(a.acc[o], kk), 6.0));
+            }
+            a.out[o] = res;
+          }
+        }
+        Epv = Ecu;
+        Fpv = Fcu;
+        Ecu = Enx;
+        Fcu = Fnx;
+      }
+    }
+    failed = __syncthreads_or(timed_out) != 0;
+  }
+  if (failed) {
+    if (tid == 0) {
+      atomicExch(a.err, 1);
+      // let the last copy issued into each ring slot land before the CTA's
+      // shared memory is released (bounded as well)
+      for (int s = 0; s < NST; ++s) {
+        int tl = -1;
+        for (int t = 0; t < nissued; ++t)
+          if (t % NST == s) tl = t;
+        if (tl >= 0) (void)mbar_wait_bounded(&bars[s], (tl / NST) & 1);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// 4-D view (x = doubles along r incl. row padding, theta rows, phi planes, variables)
+bool encode(CUtensorMap* tm, const Grid& g, const double2* base, int nvars) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[4] = {(cuuint64_t)(2 * g.PI), (cuuint64_t)g.NJ, (cuuint64_t)g.NK, (cuuint64_t)nvars};
+  cuuint64_t strides[3] = {(cuuint64_t)g.PI * 16, (cuuint64_t)g.plane * 16, (cuuint64_t)g.fs * 16};
+  cuuint32_t box[4] = {(cuuint32_t)RW, (cuuint32_t)RROWS, 1, (cuuint32_t)nvars};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+int tma_chunk(const Grid& g) {
+  const int nchunks = (g.NK + 31) / 32;
+  return (g.NK + nchunks - 1) / nchunks;
+}
+
+template <int KIND, int MK>
+int launch_one(const CUtensorMap& tm4, const CUtensorMap& tm1, const TmaArgs& a, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(tma_stage_kernel<KIND, MK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)SMEM_BYTES) != cudaSuccess)
+      return -1;
+    attr_set = true;
+  }
+  const Grid& g = a.g;
+  dim3 block(TI, TJ, 1);
+  dim3 grid((g.NI + TI - 1) / TI, (g.NJ + TJ - 1) / TJ, (g.NK + a.kchunk - 1) / a.kchunk);
+  tma_stage_kernel<KIND, MK><<<grid, block, SMEM_BYTES, st>>>(tm4, tm1, a);
+  return 0;
+}
+
+template <int KIND>
+int launch_kind(const CUtensorMap& tm4, const CUtensorMap& tm1, const TmaArgs& a, int mk, cudaStream_t st) {
+  return mk == MK_KS ? launch_one<KIND, MK_KS>(tm4, tm1, a, st) : launch_one<KIND, MK_SCHW>(tm4, tm1, a, st);
+}
+
+}  // namespace
+
+bool tma_available(const Grid& g, const double2* some_state) {
+  CUtensorMap tm;
+  return encode(&tm, g, some_state, 4) && encode(&tm, g, some_state, 1);
+}
+
+int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st) {
+  CUtensorMap tm4, tm1;
+  if (!encode(&tm4, L.g, L.in[0], 4) || !encode(&tm1, L.g, L.in[4], 1)) return -1;
+  TmaArgs a;
+  a.g = L.g;
+  a.m = L.m;
+  a.rsg = rsg;
+  for (int v = 0; v < 5; ++v) a.in[v] = L.in[v];
+  a.base = L.base;
+  a.aux4 = L.aux4;
+  a.out = L.out;
+  a.out4 = L.out4;
+  a.acc = L.acc;
+  a.skip_last_i = L.skip_last_i;
+  a.kchunk = tma_chunk(L.g);
+  a.err = err;
+  const int mk = L.metric_kind;
+  switch (kind) {
+    case ST_P2_S1A: return launch_kind<ST_P2_S1A>(tm4, tm1, a, mk, st);
+    case ST_P2_S1B: return launch_kind<ST_P2_S1B>(tm4, tm1, a, mk, st);
+    case ST_P2_S2: return launch_kind<ST_P2_S2>(tm4, tm1, a, mk, st);
+    case ST_P3_S2A: return launch_kind<ST_P3_S2A>(tm4, tm1, a, mk, st);
+    case ST_P3_S2B: return launch_kind<ST_P3_S2B>(tm4, tm1, a, mk, st);
+    case ST_P3_S3: return launch_kind<ST_P3_S3>(tm4, tm1, a, mk, st);
+    case ST_RK3_1: return launch_kind<ST_RK3_1>(tm4, tm1, a, mk, st);
+    case ST_RK3_2: return launch_kind<ST_RK3_2>(tm4, tm1, a, mk, st);
+    case ST_RK3_3: return launch_kind<ST_RK3_3>(tm4, tm1, a, mk, st);
+    case ST_RK4_1: return launch_kind<ST_RK4_1>(tm4, tm1, a, mk, st);
+    case ST_RK4_2: return launch_kind<ST_RK4_2>(tm4, tm1, a, mk, st);
+    case ST_RK4_3: return launch_kind<ST_RK4_3>(tm4, tm1, a, mk, st);
+    case ST_RK4_4: return launch_kind<ST_RK4_4>(tm4, tm1, a, mk, st);
+    default: return -1;
+  }
+}
+
+}  // namespace kg

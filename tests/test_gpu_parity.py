@@ -82,7 +82,7 @@ def test_boundary_faces_bitexact(bc):
         assert np.array_equal(dev.u, ora.get_state()), f"face {face}"
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 @pytest.mark.parametrize("method", ["pirk2", "pirk3", "rk3", "rk4"])
 @pytest.mark.parametrize("metric,bc", [("Kerr_Schild", "outflow"), ("Schw_EF", "outflow"),
                                        ("Kerr_Schild", "inflow")])
@@ -106,10 +106,12 @@ def test_steppers_bitexact(method, metric, bc, variant):
 
 @pytest.mark.parametrize("grid", [SMALL, dict(Nx=61, Ny=13, Nz=41, xmin=1.8, xmax=30.0),
                                   dict(Nx=40, Ny=12, Nz=9, xmin=1.8, xmax=20.0)])
-def test_march_ragged_tiles(grid):
+@pytest.mark.parametrize("variant", [1, 2])
+def test_march_ragged_tiles(grid, variant):
     """Grids whose r, theta and phi extents leave partial tiles and chunks
     (including a last theta tile of one row) stay bit-exact."""
     dev, ora = _pair(grid=grid)
+    dev._ck(dev._lib.kg_set_kernel_variant(dev.handle, variant))
     from kg_b200.initial_data import shell_ylm
     u0, _ = shell_ylm(grid["Nx"], grid["Ny"], grid["Nz"], grid["xmin"], grid["xmax"], seed=2, r0=5.0, sd=1.0)
     dev.u = u0
@@ -143,6 +145,7 @@ def test_c0_1000_steps_pirk2():
     g = dict(Nx=256, Ny=33, Nz=65, xmin=1.8, xmax=60.0)
     u0 = gaussian_y20(**g)
     dev = ScalarField(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], 0.25, m=0.0)
+    dev._ck(dev._lib.kg_set_kernel_variant(dev.handle, 2))
     ora = Oracle(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], CFL=0.25, m=0.0)
     dev.u = u0
     ora.set_state(u0)
