@@ -136,7 +136,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(w, threads, nx_sample=128, steps=60):
+def cpu_baseline(w, threads, nx_sample=128, steps=150):
     """The oracle (CPU restatement of the reference path) on a radial slab of the
     workload: same theta x phi grid, Nx = nx_sample cells, `steps` PIRK2 steps."""
     from oracle.oracle import Oracle, set_threads
@@ -191,7 +191,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=150)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kg", choices=["kg", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -286,7 +286,7 @@ def main():
     state_bytes = 5 * 16 * stored_points(w)
     host_u0 = torch.empty(u0.numel() * 2, dtype=torch.float64, pin_memory=True)
     host_u0.copy_(torch.view_as_real(u0).reshape(-1))
-    host_out = torch.empty_like(host_u0)
+    host_out = torch.empty(host_u0.numel(), dtype=torch.float64, pin_memory=True)
     del u0
     mass = C.c_double(0.0)
     Dp = C.POINTER(C.c_double)

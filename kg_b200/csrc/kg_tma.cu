@@ -77,6 +77,14 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, in
       : "memory");
 }
 
+// L2 prefetch of a tensor box (no shared memory, no completion to wait for)
+__device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap* tm, int c0, int c1, int c2, int c3) {
+  asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(
+                   reinterpret_cast<uint64_t>(tm)),
+               "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+               : "memory");
+}
+
 __device__ __forceinline__ double ddiv(double a, double b, double rb) {
   const double q = a * rb;
   const double r = __fma_rn(-q, b, a);
@@ -99,13 +107,15 @@ struct TmaArgs {
   int skip_last_i;
   int kchunk;
   int* err;
+  int npf;  // number of prefetch maps in use (0..2)
 };
 
 }  // namespace
 
 template <int KIND, int MK>
 __global__ void __launch_bounds__(TI * TJ, 2)
-    tma_stage_kernel(const __grid_constant__ CUtensorMap tm4, const __grid_constant__ CUtensorMap tm1, TmaArgs a) {
+    tma_stage_kernel(const __grid_constant__ CUtensorMap tm4, const __grid_constant__ CUtensorMap tm1,
+                     const __grid_constant__ CUtensorMap tp0, const __grid_constant__ CUtensorMap tp1, TmaArgs a) {
   constexpr bool PSI = (KIND != ST_P2_S1B && KIND != ST_P3_S2B);
   constexpr bool PI_ = (KIND != ST_P2_S1A && KIND != ST_P3_S2A);
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -157,12 +167,22 @@ __global__ void __launch_bounds__(TI * TJ, 2)
     mt[MT_HT * MT_N + t] = in ? ldm(M.asg_gtt, q) : 0.0;
   }
   __syncthreads();
+  // the point-wise operands (u_p, accumulator, ...) of plane k are pulled into
+  // L2 two planes ahead, so their loads in the combination hit L2
+  auto prefetch = [&](int k) {
+    if (k >= k1) return;
+    if (a.npf > 0) tma_prefetch_4d(&tp0, 2 * ii0, jj0, k, 0);
+    if (a.npf > 1) tma_prefetch_4d(&tp1, 2 * ii0, jj0, k, 0);
+  };
   int nissued = 0;  // meaningful in thread 0 only
-  if (tid == 0)
+  if (tid == 0) {
     for (int t = 0; t < NST && t < nplanes; ++t) {
       issue(t);
       nissued = t + 1;
     }
+    prefetch(k0);
+    prefetch(k0 + 1);
+  }
 
   // own-point metric
   const int q = act ? off2(g, ii, jj) : 0;
@@ -205,9 +225,12 @@ __global__ void __launch_bounds__(TI * TJ, 2)
 
   for (int i = 0; i < k1 - k0 && !failed; ++i) {
     const int k = k0 + i;
-    if (tid == 0 && i + NST < nplanes) {
-      issue(i + NST);
-      nissued = i + NST + 1;
+    if (tid == 0) {
+      if (i + NST < nplanes) {
+        issue(i + NST);
+        nissued = i + NST + 1;
+      }
+      prefetch(k + 2);
     }
     {
       const int tc = i + 1, tn = i + 2;
@@ -400,13 +423,15 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// 4-D view (x = doubles along r incl. row padding, theta rows, phi planes, variables)
-bool encode(CUtensorMap* tm, const Grid& g, const double2* base, int nvars) {
+// 4-D view (x = doubles along r incl. row padding, theta rows, phi planes, variables);
+// halo = true: the stencil box (tile + r halo 2 + theta halo 1), false: the tile
+bool encode(CUtensorMap* tm, const Grid& g, const double2* base, int nvars, bool halo = true) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[4] = {(cuuint64_t)(2 * g.PI), (cuuint64_t)g.NJ, (cuuint64_t)g.NK, (cuuint64_t)nvars};
   cuuint64_t strides[3] = {(cuuint64_t)g.PI * 16, (cuuint64_t)g.plane * 16, (cuuint64_t)g.fs * 16};
-  cuuint32_t box[4] = {(cuuint32_t)RW, (cuuint32_t)RROWS, 1, (cuuint32_t)nvars};
+  cuuint32_t box[4] = {halo ? (cuuint32_t)RW : (cuuint32_t)(2 * TI), halo ? (cuuint32_t)RROWS : (cuuint32_t)TJ, 1,
+                       (cuuint32_t)nvars};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)base, dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -419,8 +444,12 @@ int tma_chunk(const Grid& g) {
   return (g.NK + nchunks - 1) / nchunks;
 }
 
+struct Maps {
+  CUtensorMap tm4, tm1, tp0, tp1;
+};
+
 template <int KIND, int MK>
-int launch_one(const CUtensorMap& tm4, const CUtensorMap& tm1, const TmaArgs& a, cudaStream_t st) {
+int launch_one(const Maps& m, const TmaArgs& a, cudaStream_t st) {
   static bool attr_set = false;
   if (!attr_set) {
     if (cudaFuncSetAttribute(tma_stage_kernel<KIND, MK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -431,13 +460,13 @@ int launch_one(const CUtensorMap& tm4, const CUtensorMap& tm1, const TmaArgs& a,
   const Grid& g = a.g;
   dim3 block(TI, TJ, 1);
   dim3 grid((g.NI + TI - 1) / TI, (g.NJ + TJ - 1) / TJ, (g.NK + a.kchunk - 1) / a.kchunk);
-  tma_stage_kernel<KIND, MK><<<grid, block, SMEM_BYTES, st>>>(tm4, tm1, a);
+  tma_stage_kernel<KIND, MK><<<grid, block, SMEM_BYTES, st>>>(m.tm4, m.tm1, m.tp0, m.tp1, a);
   return 0;
 }
 
 template <int KIND>
-int launch_kind(const CUtensorMap& tm4, const CUtensorMap& tm1, const TmaArgs& a, int mk, cudaStream_t st) {
-  return mk == MK_KS ? launch_one<KIND, MK_KS>(tm4, tm1, a, st) : launch_one<KIND, MK_SCHW>(tm4, tm1, a, st);
+int launch_kind(const Maps& m, const TmaArgs& a, int mk, cudaStream_t st) {
+  return mk == MK_KS ? launch_one<KIND, MK_KS>(m, a, st) : launch_one<KIND, MK_SCHW>(m, a, st);
 }
 
 }  // namespace
@@ -448,8 +477,22 @@ bool tma_available(const Grid& g, const double2* some_state) {
 }
 
 int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st) {
-  CUtensorMap tm4, tm1;
-  if (!encode(&tm4, L.g, L.in[0], 4) || !encode(&tm1, L.g, L.in[4], 1)) return -1;
+  Maps mp;
+  if (!encode(&mp.tm4, L.g, L.in[0], 4) || !encode(&mp.tm1, L.g, L.in[4], 1)) return -1;
+  // point-wise operands read in the combination, prefetched into L2
+  int npf = 0;
+  const long long fs = L.g.fs;
+  auto add = [&](const double2* p, int nv) {
+    CUtensorMap* t = npf == 0 ? &mp.tp0 : &mp.tp1;
+    if (npf < 2 && p && encode(t, L.g, p, nv, false)) ++npf;
+  };
+  switch (kind) {
+    case ST_P2_S1A: case ST_P3_S2A: add(L.base, 4); break;
+    case ST_P2_S1B: add(L.base + 4 * fs, 1); break;
+    case ST_P3_S2B: add(L.base + 4 * fs, 1); add(L.aux4, 1); break;
+    case ST_RK4_2: case ST_RK4_3: case ST_RK4_4: add(L.base, 5); add(L.acc, 5); break;
+    default: add(L.base, 5); break;
+  }
   TmaArgs a;
   a.g = L.g;
   a.m = L.m;
@@ -463,21 +506,24 @@ int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err
   a.skip_last_i = L.skip_last_i;
   a.kchunk = tma_chunk(L.g);
   a.err = err;
+  a.npf = npf;
+  if (npf < 2) mp.tp1 = mp.tm1;  // unused parameter slot, never issued
+  if (npf < 1) mp.tp0 = mp.tm1;
   const int mk = L.metric_kind;
   switch (kind) {
-    case ST_P2_S1A: return launch_kind<ST_P2_S1A>(tm4, tm1, a, mk, st);
-    case ST_P2_S1B: return launch_kind<ST_P2_S1B>(tm4, tm1, a, mk, st);
-    case ST_P2_S2: return launch_kind<ST_P2_S2>(tm4, tm1, a, mk, st);
-    case ST_P3_S2A: return launch_kind<ST_P3_S2A>(tm4, tm1, a, mk, st);
-    case ST_P3_S2B: return launch_kind<ST_P3_S2B>(tm4, tm1, a, mk, st);
-    case ST_P3_S3: return launch_kind<ST_P3_S3>(tm4, tm1, a, mk, st);
-    case ST_RK3_1: return launch_kind<ST_RK3_1>(tm4, tm1, a, mk, st);
-    case ST_RK3_2: return launch_kind<ST_RK3_2>(tm4, tm1, a, mk, st);
-    case ST_RK3_3: return launch_kind<ST_RK3_3>(tm4, tm1, a, mk, st);
-    case ST_RK4_1: return launch_kind<ST_RK4_1>(tm4, tm1, a, mk, st);
-    case ST_RK4_2: return launch_kind<ST_RK4_2>(tm4, tm1, a, mk, st);
-    case ST_RK4_3: return launch_kind<ST_RK4_3>(tm4, tm1, a, mk, st);
-    case ST_RK4_4: return launch_kind<ST_RK4_4>(tm4, tm1, a, mk, st);
+    case ST_P2_S1A: return launch_kind<ST_P2_S1A>(mp, a, mk, st);
+    case ST_P2_S1B: return launch_kind<ST_P2_S1B>(mp, a, mk, st);
+    case ST_P2_S2: return launch_kind<ST_P2_S2>(mp, a, mk, st);
+    case ST_P3_S2A: return launch_kind<ST_P3_S2A>(mp, a, mk, st);
+    case ST_P3_S2B: return launch_kind<ST_P3_S2B>(mp, a, mk, st);
+    case ST_P3_S3: return launch_kind<ST_P3_S3>(mp, a, mk, st);
+    case ST_RK3_1: return launch_kind<ST_RK3_1>(mp, a, mk, st);
+    case ST_RK3_2: return launch_kind<ST_RK3_2>(mp, a, mk, st);
+    case ST_RK3_3: return launch_kind<ST_RK3_3>(mp, a, mk, st);
+    case ST_RK4_1: return launch_kind<ST_RK4_1>(mp, a, mk, st);
+    case ST_RK4_2: return launch_kind<ST_RK4_2>(mp, a, mk, st);
+    case ST_RK4_3: return launch_kind<ST_RK4_3>(mp, a, mk, st);
+    case ST_RK4_4: return launch_kind<ST_RK4_4>(mp, a, mk, st);
     default: return -1;
   }
 }
