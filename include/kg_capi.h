@@ -98,7 +98,8 @@ int kg_get_state_device(kg_solver *h, int which, double *dev_u);
 
 /* --- time steppers (MoL/lines_method_lib.f90) ---------------------------- */
 
-/* pirk2 (:271-332), nsteps consecutive calls */
+/* pirk2 (:271-332), nsteps consecutive calls.  For nsteps >= 2 the steps run
+ * as replays of a CUDA graph of two steps, captured on first use */
 int kg_pirk2(kg_solver *h, int nsteps);
 /* pirk3 (:334-408) */
 int kg_pirk3(kg_solver *h, int nsteps);
@@ -106,6 +107,8 @@ int kg_pirk3(kg_solver *h, int nsteps);
 int kg_rk3(kg_solver *h, int nsteps);
 /* rk4 (:411-474) with the same rhs */
 int kg_rk4(kg_solver *h, int nsteps);
+/* turn graph replay of multi-step calls on (default) or off */
+int kg_set_graphs(kg_solver *h, int on);
 
 /* --- RHS and boundaries (parity hooks) ----------------------------------- */
 

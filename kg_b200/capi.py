@@ -59,6 +59,7 @@ SIGNATURES = [
     ("kg_pirk3", _I, [_P, _I]),
     ("kg_rk3", _I, [_P, _I]),
     ("kg_rk4", _I, [_P, _I]),
+    ("kg_set_graphs", _I, [_P, _I]),
     ("kg_rhs", _I, [_P, _D, _D, C.c_uint]),
     ("kg_boundary", _I, [_P, C.c_uint]),
     ("kg_send_recv", _I, [_P]),

@@ -107,7 +107,8 @@ struct TmaArgs {
   int skip_last_i;
   int kchunk;
   int* err;
-  int npf;  // number of prefetch maps in use (0..2)
+  int npf;      // number of prefetch maps in use (0..2)
+  int base_in;  // the point-wise base is the stencil input itself (values already in the ring)
 };
 
 }  // namespace
@@ -333,9 +334,10 @@ __global__ void __launch_bounds__(TI * TJ, 2)
           r[4] = csub(cadd(cadd(cadd(cadd(r1, r2), r3), r4), r5), r6);
         }
         const double dt = g.dt;
+        auto B = [&](int v) { return a.base_in ? fcu[v] : ldf(a.base + v * g.fs, p); };
         if (KIND == ST_P2_S1A) {
 #pragma unroll
-          for (int v = 0; v < 4; ++v) a.out[v * g.fs + p] = cadd(ldf(a.base + v * g.fs, p), rmul(dt, r[v]));
+          for (int v = 0; v < 4; ++v) a.out[v * g.fs + p] = cadd(B(v), rmul(dt, r[v]));
         } else if (KIND == ST_P3_S2A) {
 #pragma unroll
           for (int v = 0; v < 4; ++v)
@@ -349,7 +351,7 @@ __global__ void __launch_bounds__(TI * TJ, 2)
 #pragma unroll
           for (int v = 0; v < 5; ++v) {
             const long long o = v * g.fs + p;
-            const double2 b = ldf(a.base + v * g.fs, p);
+            const double2 b = B(v);
             double2 res;
             if (KIND == ST_P2_S2) {
               res = rmul(0.5, cadd(cadd(b, fcu[v]), rmul(dt, r[v])));
@@ -486,7 +488,12 @@ int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err
     CUtensorMap* t = npf == 0 ? &mp.tp0 : &mp.tp1;
     if (npf < 2 && p && encode(t, L.g, p, nv, false)) ++npf;
   };
-  switch (kind) {
+  const long long fsl = L.g.fs;
+  int base_in = 1;
+  for (int v = 0; v < 5; ++v) base_in = base_in && (L.in[v] == L.base + v * fsl);
+  if (base_in && (kind == ST_P2_S1A || kind == ST_RK3_1 || kind == ST_RK4_1)) {
+    // nothing point-wise to prefetch except the accumulator (written, not read, in RK4 stage 1)
+  } else switch (kind) {
     case ST_P2_S1A: case ST_P3_S2A: add(L.base, 4); break;
     case ST_P2_S1B: add(L.base + 4 * fs, 1); break;
     case ST_P3_S2B: add(L.base + 4 * fs, 1); add(L.aux4, 1); break;
@@ -507,6 +514,7 @@ int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err
   a.kchunk = tma_chunk(L.g);
   a.err = err;
   a.npf = npf;
+  a.base_in = base_in && (kind == ST_P2_S1A || kind == ST_RK3_1 || kind == ST_RK4_1);
   if (npf < 2) mp.tp1 = mp.tm1;  // unused parameter slot, never issued
   if (npf < 1) mp.tp0 = mp.tm1;
   const int mk = L.metric_kind;
