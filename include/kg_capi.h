@@ -175,6 +175,30 @@ long long kg_launch_count(const kg_solver *h);
  * per point with cached neighbour loads; all give bit-identical results */
 int kg_set_kernel_variant(kg_solver *h, int variant);
 
+/* --- batched engine ------------------------------------------------------------ */
+/* No reference counterpart (the reference runs one solve per MPI job): many
+ * independent solves, each a kg_solver handle with its own grid, field mass and
+ * state, advanced together by RK4.  Each stage is ONE persistent launch over the
+ * ragged work list of all members' tiles (TMA-fed kernels), followed by one
+ * batched ghost fill; a whole step is captured once into a CUDA graph and
+ * replayed.  Members keep their own handles for state exchange and diagnostics
+ * (which wait for the batch).  All members share one metric kind. */
+typedef struct kg_batch kg_batch;
+int kg_batch_create(int device, kg_batch **out);
+int kg_batch_destroy(kg_batch *b);
+const char *kg_batch_last_error(const kg_batch *b);
+int kg_batch_add(kg_batch *b, kg_solver *h);
+int kg_batch_remove(kg_batch *b, kg_solver *h);
+int kg_batch_size(const kg_batch *b);
+/* rk4 (MoL/lines_method_lib.f90:411-474) for every member, nsteps times */
+int kg_batch_rk4(kg_batch *b, int nsteps);
+int kg_batch_synchronize(kg_batch *b);
+/* launch shape: phi planes per work item and persistent CTAs (the tuner's knobs) */
+int kg_batch_set_tuning(kg_batch *b, int kchunk, int blocks);
+int kg_batch_get_tuning(const kg_batch *b, int *kchunk, int *blocks);
+long long kg_batch_launch_count(const kg_batch *b);
+void *kg_batch_get_stream(const kg_batch *b);
+
 /* --- allocation-free diagnostic --------------------------------------------- */
 
 /* Mass_scalar = integrate(rho*sqrtg) without allocating anything.  No

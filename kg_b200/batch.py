@@ -1,0 +1,122 @@
+"""Batched engine and its launch-shape tuner.
+
+`Batch` advances many independent solves (each a `ScalarField` with its own
+grid, field mass and state) together by RK4: every stage is one persistent
+launch over the ragged work list of all members' tiles plus one batched ghost
+fill, and a step is replayed from a CUDA graph (kg_batch_* in
+include/kg_capi.h).  Members keep their handles for state exchange and
+diagnostics.
+
+`autotune` picks the two launch knobs of a batch -- phi planes per work item
+and the number of persistent CTAs -- by timing candidate shapes on scratch
+solves of the same grid shapes, so the live solves are never advanced by the
+tuning itself.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import capi
+
+
+class Batch:
+    def __init__(self, device=-1):
+        self._lib = capi.load()
+        h = C.c_void_p()
+        rc = self._lib.kg_batch_create(device, C.byref(h))
+        if rc != capi.KG_OK:
+            raise capi.KgError(rc, "kg_batch_create failed")
+        self._b = h
+        self.members = []
+
+    def _ck(self, rc):
+        if rc != capi.KG_OK:
+            raise capi.KgError(rc, self._lib.kg_batch_last_error(self._b).decode())
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self._lib.kg_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, solver):
+        self._ck(self._lib.kg_batch_add(self._b, solver.handle))
+        self.members.append(solver)
+
+    def remove(self, solver):
+        self._ck(self._lib.kg_batch_remove(self._b, solver.handle))
+        self.members.remove(solver)
+
+    def __len__(self):
+        return self._lib.kg_batch_size(self._b)
+
+    def rk4(self, nsteps=1):
+        self._ck(self._lib.kg_batch_rk4(self._b, nsteps))
+
+    def synchronize(self):
+        self._ck(self._lib.kg_batch_synchronize(self._b))
+
+    def set_tuning(self, kchunk, blocks):
+        self._ck(self._lib.kg_batch_set_tuning(self._b, int(kchunk), int(blocks)))
+
+    def tuning(self):
+        k, b = C.c_int(0), C.c_int(0)
+        self._ck(self._lib.kg_batch_get_tuning(self._b, C.byref(k), C.byref(b)))
+        return k.value, b.value
+
+    @property
+    def launch_count(self):
+        return int(self._lib.kg_batch_launch_count(self._b))
+
+    @property
+    def stream(self):
+        return self._lib.kg_batch_get_stream(self._b)
+
+
+_TUNE_CACHE = {}
+
+
+def autotune(shapes, device=-1, kchunks=(16, 24, 32, 48, 64), ctas_per_sm=(1, 2), steps=3, sms=None):
+    """Choose (kchunk, blocks) for a batch of solves with the given grid shapes.
+
+    shapes: list of (Nx, Ny, Nz).  Candidates are timed on scratch solves with
+    those shapes (zero state; the kernels' cost does not depend on the values),
+    best of `steps` graph-replayed RK4 steps each.  Results are cached per
+    sorted shape list."""
+    from .lines_method import ScalarField
+    key = tuple(sorted(shapes))
+    if key in _TUNE_CACHE:
+        return _TUNE_CACHE[key]
+    import torch
+    if sms is None:
+        sms = torch.cuda.get_device_properties(max(device, 0)).multi_processor_count
+    scratch = [ScalarField(nx, ny, nz, 1.8, 1.8 + 0.1 * nx, 0.25, device=device, n_det=2, l_max=0)
+               for (nx, ny, nz) in shapes]
+    best = None
+    for kc in kchunks:
+        for cps in ctas_per_sm:
+            b = Batch(device)
+            for s in scratch:
+                b.add(s)
+            b.set_tuning(kc, cps * sms)
+            b.rk4(2)  # builds the work list and the graph
+            b.synchronize()
+            t0 = time.perf_counter()
+            b.rk4(steps)
+            b.synchronize()
+            dt = (time.perf_counter() - t0) / steps
+            if best is None or dt < best[0]:
+                best = (dt, kc, cps * sms)
+            b.close()
+    for s in scratch:
+        s.close()
+    _TUNE_CACHE[key] = (best[1], best[2])
+    return _TUNE_CACHE[key]

@@ -94,6 +94,72 @@ void launch_ghost_fill(const Grid& g, double2* u, const double2* up, int inflow,
   ghost_z_kernel<<<(unsigned)((nz + 255) / 256), 256, 0, st>>>(g, u);
 }
 
+// ---- many solves at once (batched engine) -----------------------------------
+__global__ void ghost_xy_batch_kernel(const GhostDesc* __restrict__ d) {
+  const GhostDesc& D = d[blockIdx.y];
+  const Grid& g = D.g;
+  const long long n_rows = 6LL * g.NK * g.NI;
+  const long long n_faces = 2LL * (g.NJ - 6) * g.NK;
+  const long long total = n_rows + n_faces;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int ii, jj, k, si, sj, sk;
+    if (t < n_rows) {
+      ii = (int)(t % g.NI);
+      const long long rk = t / g.NI;
+      const int r = (int)(rk % 6);
+      k = (int)(rk / 6);
+      jj = (r < 3) ? r : (g.NJ - 6 + r);
+      si = ii;
+      sj = ghost_src_row(g, jj);
+      sk = ktarget(g, k);
+    } else {
+      const long long f = t - n_rows;
+      const int nin = g.NJ - 6;
+      jj = 3 + (int)(f % nin);
+      const long long s2 = f / nin;
+      const int side = (int)(s2 % 2);
+      k = (int)(s2 / 2);
+      ii = side ? g.NI - 1 : 0;
+      si = ii;
+      sj = jj;
+      sk = k;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+      D.u[v * g.fs + off3(g, ii, jj, k)] = xval(g, D.u + v * g.fs, D.up + v * g.fs, D.inflow, si, sj, sk);
+  }
+}
+
+__global__ void ghost_z_batch_kernel(const GhostDesc* __restrict__ d) {
+  const GhostDesc& D = d[blockIdx.y];
+  const Grid& g = D.g;
+  const long long n = (long long)g.NI * g.NJ;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int side = (int)(t / n);
+    const long long q = t % n;
+    const int ii = (int)(q % g.NI), jj = (int)(q / g.NI);
+    const int kd = side ? g.Nz : 0;
+    const int ks = side ? 1 : g.Nz - 1;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) D.u[v * g.fs + off3(g, ii, jj, kd)] = D.u[v * g.fs + off3(g, ii, jj, ks)];
+  }
+}
+
+void launch_ghost_fill_batch(const GhostDesc* d_desc, int n, long long max_rows, long long max_faces,
+                             long long max_zplanes, cudaStream_t st) {
+  if (n <= 0) return;
+  long long bx = (max_rows + max_faces + 255) / 256;
+  if (bx > 1024) bx = 1024;
+  if (bx < 1) bx = 1;
+  ghost_xy_batch_kernel<<<dim3((unsigned)bx, n), 256, 0, st>>>(d_desc);
+  long long bz = (max_zplanes + 255) / 256;
+  if (bz > 1024) bz = 1024;
+  if (bz < 1) bz = 1;
+  ghost_z_batch_kernel<<<dim3((unsigned)bz, n), 256, 0, st>>>(d_desc);
+}
+
 // ---- one reference routine at a time ---------------------------------------
 // face 0 = xL, 1 = xR, 2 = yL, 3 = yR, 4 = zL, 5 = zR
 __global__ void face_kernel(Grid g, double2* u, const double2* up, int inflow, int face) {

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -1252,5 +1253,293 @@ int kg_profile_read(kg_solver* h, double* ms, long long* launches) {
 }
 
 long long kg_launch_count(const kg_solver* h) { return h ? h->launches : 0; }
+
+}  // extern "C"
+
+// =============================================================================
+// Batched engine: many solves advanced together by RK4 with one persistent
+// launch per stage over the ragged work list of all their tiles, plus one
+// batched ghost fill, the whole step replayed from a CUDA graph.
+struct kg_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int metric_kind = -1;
+  std::vector<kg_solver*> members;
+  bool dirty = true;
+  int kchunk = 32;
+  int blocks = 0;
+  // per RK4 stage: item records and ghost descriptors (device)
+  unsigned char* ditems[4] = {nullptr, nullptr, nullptr, nullptr};
+  kg::GhostDesc* dghost[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t items_cap = 0, ghost_cap = 0;
+  int n_items[4] = {0, 0, 0, 0};
+  long long max_rows = 0, max_faces = 0, max_z = 0;
+  int* derr = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0;
+  long long launches = 0;
+  cudaEvent_t ev = nullptr;
+};
+
+#define KG_BCK(call)                                                        \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) {                                                \
+      b->err = std::string(#call) + ": " + cudaGetErrorString(e_);         \
+      return KG_ECUDA;                                                      \
+    }                                                                       \
+  } while (0)
+
+namespace {
+
+int batch_rebuild(kg_batch* b) {
+  const int n = (int)b->members.size();
+  const size_t isz = kg::batch_item_bytes();
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if ((size_t)n > b->items_cap) {
+    for (int st = 0; st < 4; ++st) {
+      if (b->ditems[st]) cudaFree(b->ditems[st]);
+      if (b->dghost[st]) cudaFree(b->dghost[st]);
+      b->ditems[st] = nullptr;
+      b->dghost[st] = nullptr;
+    }
+    size_t cap = n < 16 ? 16 : (size_t)n * 2;
+    for (int st = 0; st < 4; ++st) {
+      KG_BCK(cudaMalloc((void**)&b->ditems[st], cap * isz));
+      KG_BCK(cudaMalloc((void**)&b->dghost[st], cap * sizeof(kg::GhostDesc)));
+    }
+    b->items_cap = cap;
+  }
+  std::vector<unsigned char> hitems((size_t)n * isz);
+  std::vector<kg::GhostDesc> hg(n);
+  const int kinds[4] = {kg::ST_RK4_1, kg::ST_RK4_2, kg::ST_RK4_3, kg::ST_RK4_4};
+  b->max_rows = b->max_faces = b->max_z = 0;
+  for (int st = 0; st < 4; ++st) {
+    int item0 = 0;
+    for (int i = 0; i < n; ++i) {
+      kg_solver* h = b->members[i];
+      const Grid& g = h->g;
+      double2* R1 = h->RK;
+      double2* R2 = fld(h->RK, g, 5);
+      double2* A = fld(h->RK, g, 10);
+      kg::StageLaunch L = base_launch(h);
+      L.base = h->U;
+      L.acc = A;
+      double2* in = st == 0 ? h->U : (st == 1 ? R1 : (st == 2 ? R2 : R1));
+      double2* out = st == 0 ? R1 : (st == 1 ? R2 : (st == 2 ? R1 : h->U));
+      set_in(L, g, in, fld(in, g, 4));
+      L.out = out;
+      L.skip_last_i = (st == 3) ? (h->p.bc_rmax == KG_INFLOW) : 0;
+      const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
+      const int ni = kg::build_batch_item(hitems.data() + (size_t)i * isz, kinds[st], L, rsg, b->derr, b->kchunk,
+                                          item0);
+      if (ni < 0) {
+        b->err = "tensor-map encoding failed for a batch member";
+        return KG_ECUDA;
+      }
+      item0 += ni;
+      hg[i].g = g;
+      hg[i].u = out;
+      hg[i].up = h->U;
+      hg[i].inflow = h->p.bc_rmax == KG_INFLOW;
+      if (st == 0) {
+        b->max_rows = std::max(b->max_rows, 6LL * g.NK * g.NI);
+        b->max_faces = std::max(b->max_faces, 2LL * (g.NJ - 6) * g.NK);
+        b->max_z = std::max(b->max_z, 2LL * g.NI * g.NJ);
+      }
+    }
+    b->n_items[st] = item0;
+    KG_BCK(cudaMemcpyAsync(b->ditems[st], hitems.data(), (size_t)n * isz, cudaMemcpyHostToDevice, b->stream));
+    KG_BCK(cudaMemcpyAsync(b->dghost[st], hg.data(), (size_t)n * sizeof(kg::GhostDesc), cudaMemcpyHostToDevice,
+                           b->stream));
+  }
+  KG_BCK(cudaStreamSynchronize(b->stream));
+  b->dirty = false;
+  return KG_OK;
+}
+
+int batch_enqueue_step(kg_batch* b) {
+  const int n = (int)b->members.size();
+  const int kinds[4] = {kg::ST_RK4_1, kg::ST_RK4_2, kg::ST_RK4_3, kg::ST_RK4_4};
+  for (int st = 0; st < 4; ++st) {
+    if (kg::launch_batch_tma(kinds[st], b->metric_kind, b->ditems[st], n, b->n_items[st], b->blocks, b->stream)) {
+      b->err = "batched stage launch could not be configured";
+      return KG_ECUDA;
+    }
+    kg::launch_ghost_fill_batch(b->dghost[st], n, b->max_rows, b->max_faces, b->max_z, b->stream);
+    b->launches += 3;
+  }
+  KG_BCK(cudaGetLastError());
+  return KG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kg_batch_create(int device, kg_batch** out) {
+  if (!out) return KG_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return KG_ENODEV;
+  }
+  if (device >= 0 && (device >= ndev || cudaSetDevice(device) != cudaSuccess)) return KG_ENODEV;
+  kg_batch* b = new kg_batch();
+  cudaGetDevice(&b->device);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  b->blocks = 2 * sms;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMalloc((void**)&b->derr, 16) != cudaSuccess || cudaMemset(b->derr, 0, 16) != cudaSuccess) {
+    kg_batch_destroy(b);
+    return KG_ECUDA;
+  }
+  *out = b;
+  return KG_OK;
+}
+
+int kg_batch_destroy(kg_batch* b) {
+  if (!b) return KG_EINVAL;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (int st = 0; st < 4; ++st) {
+    if (b->ditems[st]) cudaFree(b->ditems[st]);
+    if (b->dghost[st]) cudaFree(b->dghost[st]);
+  }
+  if (b->derr) cudaFree(b->derr);
+  if (b->ev) cudaEventDestroy(b->ev);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return KG_OK;
+}
+
+const char* kg_batch_last_error(const kg_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int kg_batch_add(kg_batch* b, kg_solver* h) {
+  if (!b || !h) return KG_EINVAL;
+  if (h->device != b->device) return set_err(h, KG_EINVAL, "batch member on another device");
+  const int mk = h->p.metric == KG_SCHW_EF ? kg::MK_SCHW : kg::MK_KS;
+  if (b->metric_kind >= 0 && mk != b->metric_kind) {
+    b->err = "all members of a batch use the same metric";
+    return KG_EINVAL;
+  }
+  for (kg_solver* m : b->members)
+    if (m == h) return KG_OK;
+  int rc;
+  if ((rc = ensure(h, &h->RK, 15))) return rc;
+  if (!kg::tma_available(h->g, h->U)) {
+    b->err = "tensor maps unavailable for this grid";
+    return KG_EINVAL;
+  }
+  b->metric_kind = mk;
+  b->members.push_back(h);
+  b->dirty = true;
+  return KG_OK;
+}
+
+int kg_batch_remove(kg_batch* b, kg_solver* h) {
+  if (!b || !h) return KG_EINVAL;
+  for (size_t i = 0; i < b->members.size(); ++i)
+    if (b->members[i] == h) {
+      // a member leaving must not have batch work in flight on its buffers
+      KG_BCK(cudaStreamSynchronize(b->stream));
+      b->members.erase(b->members.begin() + (long)i);
+      b->dirty = true;
+      if (b->members.empty()) b->metric_kind = -1;
+      return KG_OK;
+    }
+  return KG_EINVAL;
+}
+
+int kg_batch_size(const kg_batch* b) { return b ? (int)b->members.size() : 0; }
+
+// RK4 (MoL/lines_method_lib.f90:411-474) for every member, nsteps times.
+int kg_batch_rk4(kg_batch* b, int nsteps) {
+  if (!b || nsteps < 0) return KG_EINVAL;
+  if (b->members.empty() || nsteps == 0) return KG_OK;
+  int rc;
+  if (b->dirty && (rc = batch_rebuild(b))) return rc;
+  // order after each member's own pending work
+  for (kg_solver* h : b->members) {
+    KG_BCK(cudaEventRecord(b->ev, h->stream));
+    KG_BCK(cudaStreamWaitEvent(b->stream, b->ev, 0));
+  }
+  if (!b->graph) {
+    // first step direct (kernel attributes), then capture one step
+    const long long l0 = b->launches;
+    if ((rc = batch_enqueue_step(b))) return rc;
+    for (kg_solver* h : b->members) h->t = h->t + h->dt;
+    nsteps -= 1;
+    cudaGraph_t graph;
+    KG_BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const long long l1 = b->launches;
+    rc = batch_enqueue_step(b);
+    cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
+    b->graph_launches = b->launches - l1;
+    b->launches = l1;
+    if (rc) return rc;
+    if (ec != cudaSuccess) {
+      b->err = std::string("batch graph capture: ") + cudaGetErrorString(ec);
+      return KG_ECUDA;
+    }
+    ec = cudaGraphInstantiate(&b->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ec != cudaSuccess) {
+      b->graph = nullptr;
+      b->err = std::string("batch graph instantiate: ") + cudaGetErrorString(ec);
+      return KG_ECUDA;
+    }
+    (void)l0;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    KG_BCK(cudaGraphLaunch(b->graph, b->stream));
+    b->launches += b->graph_launches;
+    for (kg_solver* h : b->members) h->t = h->t + h->dt;
+  }
+  // members' later work waits for the batch
+  KG_BCK(cudaEventRecord(b->ev, b->stream));
+  for (kg_solver* h : b->members) KG_BCK(cudaStreamWaitEvent(h->stream, b->ev, 0));
+  return KG_OK;
+}
+
+int kg_batch_synchronize(kg_batch* b) {
+  if (!b) return KG_EINVAL;
+  KG_BCK(cudaStreamSynchronize(b->stream));
+  int f = 0;
+  KG_BCK(cudaMemcpy(&f, b->derr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (f) {
+    b->err = "a device wait ran out in a batched launch";
+    return KG_ETIMEOUT;
+  }
+  return KG_OK;
+}
+
+int kg_batch_set_tuning(kg_batch* b, int kchunk, int blocks) {
+  if (!b || kchunk < 1 || blocks < 1) return KG_EINVAL;
+  if (kchunk != b->kchunk || blocks != b->blocks) {
+    b->kchunk = kchunk;
+    b->blocks = blocks;
+    b->dirty = true;
+  }
+  return KG_OK;
+}
+
+int kg_batch_get_tuning(const kg_batch* b, int* kchunk, int* blocks) {
+  if (!b) return KG_EINVAL;
+  if (kchunk) *kchunk = b->kchunk;
+  if (blocks) *blocks = b->blocks;
+  return KG_OK;
+}
+
+long long kg_batch_launch_count(const kg_batch* b) { return b ? b->launches : 0; }
+
+void* kg_batch_get_stream(const kg_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 }  // extern "C"

@@ -44,6 +44,19 @@ void launch_stage_march(int kind, const StageLaunch& L, const double* rsg, cudaS
 int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st);
 // true when the driver can encode the tensor maps the TMA form needs for this grid
 bool tma_available(const Grid& g, const double2* some_state);
+// batched (multi-solve) persistent launches of the TMA stage kernel
+size_t batch_item_bytes();
+int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rsg, int* err, int kchunk, int item0);
+int launch_batch_tma(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks, cudaStream_t st);
+// batched ghost fill: one launch pair for many solves
+struct GhostDesc {
+  Grid g;
+  double2* u;
+  const double2* up;
+  int inflow;
+};
+void launch_ghost_fill_batch(const GhostDesc* d_desc, int n, long long max_rows, long long max_faces,
+                             long long max_zplanes, cudaStream_t st);
 void launch_rhs(const Grid& g, const Metric& m, int metric_kind, const double2* const in[5], double2* out,
                 unsigned mask, cudaStream_t st);
 

@@ -25,6 +25,7 @@
 // (bounded) for its own copies and returns; the host reports KG_ETIMEOUT.
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cstring>
 #include "kg_device.cuh"
 #include "kg_internal.h"
 
@@ -41,7 +42,7 @@ constexpr int NST = 3;                        // ring depth
 constexpr int MW = TI + 2 * RH, MH = TJ + 2;  // metric tile
 constexpr int MT_N = MW * MH;
 enum { MT_AL = 0, MT_BE, MT_A, MT_GRR, MT_GRP, MT_SG, MT_HT, MT_COUNT };
-constexpr size_t SMEM_BYTES = (size_t)NST * STAGE_B + (size_t)MT_COUNT * MT_N * 8 + 64;
+constexpr size_t SMEM_BYTES = (size_t)NST * STAGE_B + (size_t)MT_COUNT * MT_N * 8 + 64 + 128;
 constexpr long long WAIT_LIMIT = 1LL << 24;
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -113,25 +114,31 @@ struct TmaArgs {
 
 }  // namespace
 
+// one solve of a batched launch (kept in device memory; tensor maps 64-byte aligned)
+struct alignas(64) BatchItem {
+  CUtensorMap tm4, tm1, tp0, tp1;
+  TmaArgs a;
+  int tiles_x, tiles_y, item0, n_items;
+};
+
+// One work item: a tile of (r, theta) columns through one chunk of phi planes.
+// `tb` counts the planes this CTA has already pulled through its ring (ring
+// slot and mbarrier parity continue across items in the persistent kernel).
+// Returns the number of planes consumed, or -1 when a bounded wait ran out.
 template <int KIND, int MK>
-__global__ void __launch_bounds__(TI * TJ, 2)
-    tma_stage_kernel(const __grid_constant__ CUtensorMap tm4, const __grid_constant__ CUtensorMap tm1,
-                     const __grid_constant__ CUtensorMap tp0, const __grid_constant__ CUtensorMap tp1, TmaArgs a) {
+__device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtensorMap* tm1p, const CUtensorMap* tp0p,
+                                          const CUtensorMap* tp1p, const TmaArgs& a, int bx, int by, int bz,
+                                          double* ring, double* mt, uint64_t* bars, uint32_t tb) {
   constexpr bool PSI = (KIND != ST_P2_S1B && KIND != ST_P3_S2B);
   constexpr bool PI_ = (KIND != ST_P2_S1A && KIND != ST_P3_S2A);
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  double* ring = reinterpret_cast<double*>(smem_raw);
-  double* mt = ring + (size_t)NST * STAGE_D;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
-
   const Grid& g = a.g;
   const Metric& M = a.m;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TI + tx;
-  const int ii0 = blockIdx.x * TI, jj0 = blockIdx.y * TJ;
+  const int ii0 = bx * TI, jj0 = by * TJ;
   const int ii = ii0 + tx, jj = jj0 + ty;
   const bool act = (ii < g.NI) && (jj < g.NJ);
-  const int k0 = blockIdx.z * a.kchunk;
-  if (k0 >= g.NK) return;
+  const int k0 = bz * a.kchunk;
+  if (k0 >= g.NK) return 0;
   const int k1 = min(k0 + a.kchunk, g.NK);
   const int nplanes = (k1 - k0) + 2;  // previous, the chunk, next
   auto plane_of = [&](int t) -> int {
@@ -139,20 +146,18 @@ __global__ void __launch_bounds__(TI * TJ, 2)
     if (t <= k1 - k0) return k0 + t - 1;
     return (k1 - 1 == g.Nz) ? 2 : k1;
   };
+  auto slot = [&](int t) -> int { return (int)((tb + (uint32_t)t) % NST); };
+  auto parity = [&](int t) -> uint32_t { return ((tb + (uint32_t)t) / NST) & 1u; };
   auto issue = [&](int t) {
-    const int s = t % NST;
+    const int s = slot(t);
     uint64_t* b = &bars[s];
     double* dst = ring + (size_t)s * STAGE_D;
     mbar_expect_tx(b, STAGE_B);
     const int z = plane_of(t);
-    tma_load_4d(dst, &tm4, 2 * (ii0 - RH), jj0 - 1, z, 0, b);
-    tma_load_4d(dst + 4 * FIELD_D, &tm1, 2 * (ii0 - RH), jj0 - 1, z, 0, b);
+    tma_load_4d(dst, tm4p, 2 * (ii0 - RH), jj0 - 1, z, 0, b);
+    tma_load_4d(dst + 4 * FIELD_D, tm1p, 2 * (ii0 - RH), jj0 - 1, z, 0, b);
   };
 
-  if (tid == 0) {
-    for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
   // metric tile (phi-independent), zero outside the array
   for (int t = tid; t < MT_N; t += TI * TJ) {
     const int mx = t % MW, my = t / MW;
@@ -172,8 +177,8 @@ __global__ void __launch_bounds__(TI * TJ, 2)
   // L2 two planes ahead, so their loads in the combination hit L2
   auto prefetch = [&](int k) {
     if (k >= k1) return;
-    if (a.npf > 0) tma_prefetch_4d(&tp0, 2 * ii0, jj0, k, 0);
-    if (a.npf > 1) tma_prefetch_4d(&tp1, 2 * ii0, jj0, k, 0);
+    if (a.npf > 0) tma_prefetch_4d(tp0p, 2 * ii0, jj0, k, 0);
+    if (a.npf > 1) tma_prefetch_4d(tp1p, 2 * ii0, jj0, k, 0);
   };
   int nissued = 0;  // meaningful in thread 0 only
   if (tid == 0) {
@@ -216,9 +221,9 @@ __global__ void __launch_bounds__(TI * TJ, 2)
 
   int timed_out = 0;
   double2 Epv = c2(0, 0), Fpv = c2(0, 0), Ecu = c2(0, 0), Fcu = c2(0, 0);
-  if (!mbar_wait_bounded(&bars[0], 0)) timed_out = 1;
+  if (!mbar_wait_bounded(&bars[slot(0)], parity(0))) timed_out = 1;
   if (act && !timed_out) {
-    const double* st = ring;
+    const double* st = ring + (size_t)slot(0) * STAGE_D;
     if (PSI) Epv = phiE(st);
     if (PI_) Fpv = phiF(st);
   }
@@ -235,12 +240,12 @@ __global__ void __launch_bounds__(TI * TJ, 2)
     }
     {
       const int tc = i + 1, tn = i + 2;
-      const bool okc = mbar_wait_bounded(&bars[tc % NST], (tc / NST) & 1);
-      const bool okn = okc && mbar_wait_bounded(&bars[tn % NST], (tn / NST) & 1);
+      const bool okc = mbar_wait_bounded(&bars[slot(tc)], parity(tc));
+      const bool okn = okc && mbar_wait_bounded(&bars[slot(tn)], parity(tn));
       if (!okn) timed_out = 1;
       if (act && !timed_out) {
-        const double* cu = ring + (size_t)(tc % NST) * STAGE_D;
-        const double* nx = ring + (size_t)(tn % NST) * STAGE_D;
+        const double* cu = ring + (size_t)slot(tc) * STAGE_D;
+        const double* nx = ring + (size_t)slot(tn) * STAGE_D;
         if (i == 0) {
           if (PSI) Ecu = phiE(cu);
           if (PI_) Fcu = phiF(cu);
@@ -398,11 +403,80 @@ __global__ void __launch_bounds__(TI * TJ, 2)
       for (int s = 0; s < NST; ++s) {
         int tl = -1;
         for (int t = 0; t < nissued; ++t)
-          if (t % NST == s) tl = t;
-        if (tl >= 0) (void)mbar_wait_bounded(&bars[s], (tl / NST) & 1);
+          if (slot(t) == s) tl = t;
+        if (tl >= 0) (void)mbar_wait_bounded(&bars[s], parity(tl));
       }
     }
     __syncthreads();
+    return -1;
+  }
+  return nplanes;
+}
+
+// the TMA destinations must start on 128-byte boundaries of the shared window
+__device__ __forceinline__ unsigned char* align128(unsigned char* p) {
+  const uint32_t a = saddr(p);
+  return p + ((128u - (a & 127u)) & 127u);
+}
+
+__device__ __forceinline__ void init_ring_barriers(uint64_t* bars) {
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+template <int KIND, int MK>
+__global__ void __launch_bounds__(TI * TJ, 2)
+    tma_stage_kernel(const __grid_constant__ CUtensorMap tm4, const __grid_constant__ CUtensorMap tm1,
+                     const __grid_constant__ CUtensorMap tp0, const __grid_constant__ CUtensorMap tp1, TmaArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  double* ring = reinterpret_cast<double*>(align128(smem_raw));
+  double* mt = ring + (size_t)NST * STAGE_D;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
+  if ((int)blockIdx.z * a.kchunk >= a.g.NK) return;
+  init_ring_barriers(bars);
+  (void)stage_item<KIND, MK>(&tm4, &tm1, &tp0, &tp1, a, blockIdx.x, blockIdx.y, blockIdx.z, ring, mt, bars, 0u);
+}
+
+// ---- persistent kernel over many solves -------------------------------------
+// Every solve of a batch contributes tiles_x * tiles_y * chunks work items; a
+// CTA walks the ragged list item = blockIdx.x, blockIdx.x + gridDim.x, ...
+// and runs each with the solve's own grid, metric, buffers and tensor maps.
+template <int KIND, int MK>
+__global__ void __launch_bounds__(TI * TJ, 2) tma_batch_kernel(const BatchItem* __restrict__ solves, int n_solves,
+                                                                 int n_items) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  double* ring = reinterpret_cast<double*>(align128(smem_raw));
+  double* mt = ring + (size_t)NST * STAGE_D;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
+  __shared__ TmaArgs sa;
+  __shared__ int s_bx, s_by, s_bz, s_solve;
+  init_ring_barriers(bars);
+  uint32_t tb = 0;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      int lo = 0, hi = n_solves - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (solves[mid].item0 <= item) lo = mid;
+        else hi = mid - 1;
+      }
+      const BatchItem& B = solves[lo];
+      const int local = item - B.item0;
+      s_solve = lo;
+      s_bx = local % B.tiles_x;
+      s_by = (local / B.tiles_x) % B.tiles_y;
+      s_bz = local / (B.tiles_x * B.tiles_y);
+      sa = B.a;
+    }
+    __syncthreads();
+    const BatchItem& B = solves[s_solve];
+    const int used = stage_item<KIND, MK>(&B.tm4, &B.tm1, &B.tp0, &B.tp1, sa, s_bx, s_by, s_bz, ring, mt, bars, tb);
+    if (used < 0) break;
+    tb += (uint32_t)used;
+    __syncthreads();  // sa and the item indices are rewritten for the next item
   }
 }
 
@@ -472,6 +546,92 @@ int launch_kind(const Maps& m, const TmaArgs& a, int mk, cudaStream_t st) {
 }
 
 }  // namespace
+
+size_t batch_item_bytes() { return sizeof(BatchItem); }
+
+// fill one solve's item record for a batched launch of stage `kind`
+int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rsg, int* err, int kchunk,
+                     int item0) {
+  BatchItem* B = reinterpret_cast<BatchItem*>(dst);
+  memset(B, 0, sizeof(BatchItem));
+  if (!encode(&B->tm4, L.g, L.in[0], 4) || !encode(&B->tm1, L.g, L.in[4], 1)) return -1;
+  const long long fsl = L.g.fs;
+  int base_in = 1;
+  for (int v = 0; v < 5; ++v) base_in = base_in && (L.in[v] == L.base + v * fsl);
+  base_in = base_in && (kind == ST_P2_S1A || kind == ST_RK3_1 || kind == ST_RK4_1);
+  int npf = 0;
+  auto add = [&](const double2* p, int nv) {
+    CUtensorMap* t = npf == 0 ? &B->tp0 : &B->tp1;
+    if (npf < 2 && p && encode(t, L.g, p, nv, false)) ++npf;
+  };
+  if (!base_in) {
+    switch (kind) {
+      case ST_P2_S1A: case ST_P3_S2A: add(L.base, 4); break;
+      case ST_P2_S1B: add(L.base + 4 * fsl, 1); break;
+      case ST_P3_S2B: add(L.base + 4 * fsl, 1); add(L.aux4, 1); break;
+      case ST_RK4_2: case ST_RK4_3: case ST_RK4_4: add(L.base, 5); add(L.acc, 5); break;
+      default: add(L.base, 5); break;
+    }
+  }
+  if (npf < 2) B->tp1 = B->tm1;
+  if (npf < 1) B->tp0 = B->tm1;
+  TmaArgs& a = B->a;
+  a.g = L.g;
+  a.m = L.m;
+  a.rsg = rsg;
+  for (int v = 0; v < 5; ++v) a.in[v] = L.in[v];
+  a.base = L.base;
+  a.aux4 = L.aux4;
+  a.out = L.out;
+  a.out4 = L.out4;
+  a.acc = L.acc;
+  a.skip_last_i = L.skip_last_i;
+  a.kchunk = kchunk;
+  a.err = err;
+  a.npf = npf;
+  a.base_in = base_in;
+  B->tiles_x = (L.g.NI + TI - 1) / TI;
+  B->tiles_y = (L.g.NJ + TJ - 1) / TJ;
+  const int chunks = (L.g.NK + kchunk - 1) / kchunk;
+  B->item0 = item0;
+  B->n_items = B->tiles_x * B->tiles_y * chunks;
+  return B->n_items;
+}
+
+namespace {
+template <int KIND, int MK>
+int batch_one(const void* items, int n_solves, int n_items, int blocks, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(tma_batch_kernel<KIND, MK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)SMEM_BYTES) != cudaSuccess)
+      return -1;
+    attr_set = true;
+  }
+  if (n_items <= 0) return 0;
+  tma_batch_kernel<KIND, MK><<<blocks, dim3(TI, TJ, 1), SMEM_BYTES, st>>>(
+      reinterpret_cast<const BatchItem*>(items), n_solves, n_items);
+  return 0;
+}
+template <int KIND>
+int batch_kind(const void* items, int n_solves, int n_items, int blocks, int mk, cudaStream_t st) {
+  return mk == MK_KS ? batch_one<KIND, MK_KS>(items, n_solves, n_items, blocks, st)
+                     : batch_one<KIND, MK_SCHW>(items, n_solves, n_items, blocks, st);
+}
+}  // namespace
+
+int launch_batch_tma(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks, cudaStream_t st) {
+  switch (kind) {
+    case ST_P2_S1A: return batch_kind<ST_P2_S1A>(d_items, n_solves, n_items, blocks, mk, st);
+    case ST_P2_S1B: return batch_kind<ST_P2_S1B>(d_items, n_solves, n_items, blocks, mk, st);
+    case ST_P2_S2: return batch_kind<ST_P2_S2>(d_items, n_solves, n_items, blocks, mk, st);
+    case ST_RK4_1: return batch_kind<ST_RK4_1>(d_items, n_solves, n_items, blocks, mk, st);
+    case ST_RK4_2: return batch_kind<ST_RK4_2>(d_items, n_solves, n_items, blocks, mk, st);
+    case ST_RK4_3: return batch_kind<ST_RK4_3>(d_items, n_solves, n_items, blocks, mk, st);
+    case ST_RK4_4: return batch_kind<ST_RK4_4>(d_items, n_solves, n_items, blocks, mk, st);
+    default: return -1;
+  }
+}
 
 bool tma_available(const Grid& g, const double2* some_state) {
   CUtensorMap tm;
