@@ -155,6 +155,32 @@ def cpu_baseline(w, threads, nx_sample=128, steps=150):
     return gpsu, dt, f"PIRK2 x{steps} on the Nx={Nx} radial slab of the workload grid ({Nx}x{w['Ny']}x{w['Nz']})"
 
 
+SERVE_DESC = ("scaled serving workload: Poisson arrivals at 60/s, Nr ~ U{128..512 step 64} on r in "
+              "[1.8, 1.8+0.1 Nr], Ntheta in {16, 32}, Nphi = 2 Ntheta, m ~ U[0, 0.5], shell r0 ~ U[6, 15], "
+              "sigma ~ U[0.8, 2], c_lm (l<=4) N(0, 1e-4), RK4, steps log-uniform [100, 1000] (multiples of 10), "
+              "l<=8 waveform at r_ext = 0.8 r_max every 10 steps, 160 GB HBM admission budget; the full serving "
+              "description (100 req/s for 120 s, Nr up to 4096, up to 20000 steps) offers several hundred times "
+              "one GPU's HBM roofline, so it is scaled down in count, grid and steps")
+
+
+def serve_leg(count, device):
+    """plain FP64 (one solve at a time) vs continuous batching on the same requests"""
+    from kg_b200.serve import Server, draw_requests, waveform_error
+    from kg_b200.batch import autotune
+    reqs = draw_requests(seed=20240602, rate=60.0, count=count, nr=(128, 512), nr_step=64, ntheta=(16, 32),
+                         steps=(100, 1000), quantum=10)
+    shapes = sorted({(r.grid()["Nx"], r.grid()["Ny"], r.grid()["Nz"]) for r in reqs})
+    tune = autotune(shapes[:: max(1, len(shapes) // 6)], device=device, kchunks=(16, 32, 64), steps=2)
+    batched = Server(mode="batched", device=device, tuning=tune).run(reqs)
+    plain = Server(mode="plain", device=device).run(reqs)
+    strip = lambda d: {k: d[k] for k in ("completed", "wall_s", "solves_per_s", "p50_s", "p99_s") if k in d}
+    out = {"workload": SERVE_DESC, "requests": count, "plain_fp64": strip(plain),
+           "batched_fp64": dict(strip(batched), peak_live=batched.get("peak_live"), tuning=list(tune)),
+           "speedup_solves_per_s": batched["solves_per_s"] / plain["solves_per_s"],
+           "waveform_rel_l2_batched_vs_plain": waveform_error(batched, plain)}
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -199,6 +225,8 @@ def main():
                     help="Nx,Ny,Nz override (profiling captures of a smaller case); r range scales with Nx")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and other-stepper legs")
     ap.add_argument("--variant", type=int, default=None, help="stage-kernel form (kg_set_kernel_variant)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-count", type=int, default=120)
     args = ap.parse_args()
     if args.grid:
         nx, ny, nz = (int(v) for v in args.grid.split(","))
@@ -338,6 +366,9 @@ def main():
                 "value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": (state_bytes + 8 * args.steps) / args.steps},
             "gpu_launches": int(launches), "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_serve and not args.grid:
+        mol.close()
+        line["serving"] = serve_leg(args.serve_count, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, secs, sample = cpu_baseline(w, threads)

@@ -151,6 +151,9 @@ int kg_proyector_detectors(kg_solver *h, double *host_alm);
 /* diagnostic(index) (:185-217): density is not recomputed (as in the
  * reference); every `save` steps currents and a_lm are refreshed on device. */
 int kg_diagnostic(kg_solver *h, int index, double *mass_out);
+/* replace the detector radii (the reference places them at MoL/diagnostic_lib.f90:124-134);
+ * each radius is located on the vertex grid the same way (main/global_numbers.f90:152-164) */
+int kg_set_detectors(kg_solver *h, int n, const double *radii);
 /* detector radii and vertex indices (1-based) */
 int kg_get_detectors(kg_solver *h, double *r_det, int *index_det);
 /* sph_harmonics (tools/FFT_sph.f90:282-336) on the vertex grid:

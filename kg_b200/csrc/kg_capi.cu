@@ -389,15 +389,25 @@ double norm_plm(int l, int m, double theta) {
 
 // detectors (MoL/diagnostic_lib.f90:124-134, main/global_numbers.f90:152-164)
 // and the domain_to_sph index search (tools/FFT_sph.f90:553-613)
-int build_detectors(kg_solver* h) {
+// radii = nullptr: the reference's detector placement
+int build_detectors(kg_solver* h, const double* radii = nullptr) {
   const int n = h->n_det, Ny = h->Ny, Nz = h->Nz, L = h->L;
   h->r_det.assign(n, 0.0);
   h->index_det.assign(n, 0);
   h->active.assign(n, 0);
-  h->r_det[0] = (1.0 + std::sqrt(1.0 - h->p.a * h->p.a));
-  h->r_det[n - 1] = h->p.xmax * 0.99;
-  for (int d = 2; d <= n - 1; ++d)
-    h->r_det[d - 1] = h->r_det[0] + (h->r_det[n - 1] - h->r_det[0]) / (double)n * (double)(d - 1);
+  if (radii) {
+    for (int d = 0; d < n; ++d) h->r_det[d] = radii[d];
+  } else {
+    h->r_det[0] = (1.0 + std::sqrt(1.0 - h->p.a * h->p.a));
+    h->r_det[n - 1] = h->p.xmax * 0.99;
+    for (int d = 2; d <= n - 1; ++d)
+      h->r_det[d - 1] = h->r_det[0] + (h->r_det[n - 1] - h->r_det[0]) / (double)n * (double)(d - 1);
+  }
+  for (void** p : {(void**)&h->d_int, (void**)&h->d_dbl, (void**)&h->shells, (void**)&h->alm, (void**)&h->flux})
+    if (*p) {
+      cudaFree(*p);
+      *p = nullptr;
+    }
   auto rv = [&](int iv) { return h->xmin + (double)(iv - 1) * h->dx; };
   for (int d = 0; d < n; ++d) {
     for (int i = 1; i <= h->Nx - 1; ++i)
@@ -1181,6 +1191,16 @@ int kg_diagnostic(kg_solver* h, int index, double* mass_out) {
     KG_CK(cudaGetLastError());
   }
   if (mass_out) return kg_mass_scalar(h, mass_out);
+  return KG_OK;
+}
+
+int kg_set_detectors(kg_solver* h, int n, const double* radii) {
+  if (!h || n < 1 || !radii) return KG_EINVAL;
+  KG_CK(cudaStreamSynchronize(h->stream));
+  h->n_det = n;
+  int rc = build_detectors(h, radii);
+  if (rc) return rc;
+  KG_CK(cudaStreamSynchronize(h->stream));
   return KG_OK;
 }
 

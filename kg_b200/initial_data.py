@@ -152,4 +152,7 @@ def shell_ylm_device(Nx, Ny, Nz, xmin, xmax, seed, device, lmax=4, sd=1.0e-4, si
     d[0] = (-phi[Nz - 2] + phi[1]) * res
     d[1:-1] = (-phi[:-2] + phi[2:]) * res
     d[Nz] = (-phi[2] + phi[Nz - 1]) * res
+    if u.is_cuda:
+        # the solver reads the tensor on its own stream
+        torch.cuda.current_stream(u.device).synchronize()
     return u, r0

@@ -243,6 +243,13 @@ class ScalarField(LinesMethod):
         self.Mass_scalar = out.value
         return self.Mass_scalar
 
+    def set_detectors(self, radii):
+        r = np.ascontiguousarray(radii, dtype=np.float64)
+        self._ck(self._lib.kg_set_detectors(self._h, len(r), _dp(r)))
+        self.n_det = len(r)
+        self.momentum = np.zeros((self.n_det, 3))
+        self.alm = np.zeros((self.n_det, 2 * self.l_max + 1, self.l_max + 1), np.complex128)
+
     def detectors(self):
         r = np.zeros(self.n_det)
         idx = np.zeros(self.n_det, np.int32)

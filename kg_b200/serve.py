@@ -1,0 +1,219 @@
+"""Serving loop: continuous batching of Klein-Gordon solves on one GPU.
+
+Requests (grid size, field mass, initial data, step count) arrive over time;
+the server admits them against an HBM budget as memory frees up, keeps every
+live solve's state on the device, advances all live solves together through
+the batched engine (one persistent launch per RK4 stage over all of them, a
+step replayed from a CUDA graph), samples each solve's l <= l_max waveform
+a_lm(t) at r_ext = 0.8 r_max every `save_every` steps, and retires a solve --
+returning its waveform -- as soon as it has run its steps.  New arrivals join
+between batch quanta, so requests that arrive while others are on the GPU
+overlap with them.
+
+`mode="plain"` serves the same requests one at a time through the single-solve
+path (kg_rk4 on its own handle), the baseline the batched form is compared
+with.
+
+The reference has no serving layer (one MPI job per solve); the solve itself
+is the reference's RK4 path (MoL/lines_method_lib.f90:411-474) and the
+waveform is its detector projection (MoL/diagnostic_lib.f90:231-250).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float       # seconds after the start of the run
+    Nr: int              # radial cells
+    Ntheta: int          # theta cells (reference Ny = Ntheta + 1, Nz = 2 Ntheta + 1)
+    m: float             # field mass
+    seed: int            # initial-data seed (shell centre, width, c_lm)
+    steps: int
+    r0: float = 10.0
+    sigma: float = 1.5
+
+    def grid(self):
+        return dict(Nx=self.Nr, Ny=self.Ntheta + 1, Nz=2 * self.Ntheta + 1, xmin=1.8, xmax=1.8 + 0.1 * self.Nr)
+
+    def points(self):
+        g = self.grid()
+        return (g["Nx"] + 5) * (g["Ny"] + 5) * (g["Nz"] + 1)
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float
+    done: float
+    steps: int
+    times: np.ndarray = field(repr=False)
+    alm: np.ndarray = field(repr=False)   # (samples, 2L+1, L+1) complex
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+def draw_requests(seed, rate, count, nr=(128, 1024), nr_step=64, ntheta=(16, 32, 64), steps=(500, 20000),
+                  mass=(0.0, 0.5), r0=(6.0, 15.0), sigma=(0.8, 2.0), quantum=10):
+    """Poisson arrivals at `rate` per second; parameters drawn as in the batched
+    benchmark description (Nr uniform on a grid of nr_step, Ntheta from a set,
+    Nphi = 2 Ntheta, log-uniform step counts rounded up to the quantum)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += rng.exponential(1.0 / rate)
+        n_r = int(rng.choice(np.arange(nr[0], nr[1] + 1, nr_step)))
+        nt = int(rng.choice(ntheta))
+        st = int(math.exp(rng.uniform(math.log(steps[0]), math.log(steps[1]))))
+        st = max(quantum, int(math.ceil(st / quantum)) * quantum)
+        out.append(Request(rid=i, arrival=t, Nr=n_r, Ntheta=nt, m=float(rng.uniform(*mass)),
+                           seed=int(rng.integers(1 << 30)), steps=st, r0=float(rng.uniform(*r0)),
+                           sigma=float(rng.uniform(*sigma))))
+    return out
+
+
+def _make_solve(req, l_max, device):
+    from .lines_method import ScalarField
+    from .initial_data import shell_ylm_device
+    g = req.grid()
+    s = ScalarField(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], 0.25, m=req.m, l_max=l_max, n_det=2,
+                    device=device)
+    u0, _ = shell_ylm_device(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], seed=req.seed,
+                             device=f"cuda:{max(device, 0)}", sigma=req.sigma, r0_range=(req.r0, req.r0))
+    s._ck(s._lib.kg_set_state_device(s.handle, 0, C.c_void_p(u0.data_ptr())))
+    s.synchronize()
+    del u0
+    r_max = s.r_max
+    s.set_detectors([0.8 * r_max, 0.8 * r_max])
+    return s
+
+
+def _bytes_estimate(req):
+    """device bytes of a live solve: u (5 copies of a variable), RK4 stage
+    buffers and accumulator (15), staging for the layout conversion (5),
+    tables and detector data (small)."""
+    return req.points() * 16 * 25 + (64 << 20)
+
+
+class Server:
+    def __init__(self, mode="batched", hbm_budget=160e9, save_every=10, l_max=8, device=0, tuning=None,
+                 max_live=4096):
+        if mode not in ("batched", "plain"):
+            raise ValueError("mode is 'batched' or 'plain'")
+        self.mode, self.budget, self.q, self.l_max, self.device = mode, hbm_budget, save_every, l_max, device
+        self.tuning, self.max_live = tuning, max_live
+
+    def _sample(self, s):
+        a = s.proyector_detectors()
+        return a[0].copy()
+
+    def run(self, requests):
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        if self.mode == "plain":
+            return self._run_plain(reqs)
+        return self._run_batched(reqs)
+
+    def _run_plain(self, reqs):
+        results = []
+        t0 = time.perf_counter()
+        for r in reqs:
+            now = time.perf_counter() - t0
+            if r.arrival > now:
+                time.sleep(r.arrival - now)
+            admitted = time.perf_counter() - t0
+            s = _make_solve(r, self.l_max, self.device)
+            ts, alms = [], []
+            done_steps = 0
+            while done_steps < r.steps:
+                s.rk4(nsteps=self.q)
+                done_steps += self.q
+                alms.append(self._sample(s))
+                ts.append(s.t)
+            done = time.perf_counter() - t0
+            results.append(Result(r.rid, r.arrival, admitted, done, r.steps, np.array(ts), np.array(alms)))
+            s.close()
+        return self._summary(results, time.perf_counter() - t0)
+
+    def _run_batched(self, reqs):
+        from .batch import Batch
+        batch = Batch(self.device)
+        if self.tuning:
+            batch.set_tuning(*self.tuning)
+        pending = deque()
+        live = []  # [req, solve, steps_done, admitted, times, alms]
+        used = 0.0
+        results = []
+        i_next = 0
+        t0 = time.perf_counter()
+        peak_live = 0
+        while i_next < len(reqs) or pending or live:
+            now = time.perf_counter() - t0
+            while i_next < len(reqs) and reqs[i_next].arrival <= now:
+                pending.append(reqs[i_next])
+                i_next += 1
+            # admission against the HBM budget, first come first served
+            while pending and len(live) < self.max_live and used + _bytes_estimate(pending[0]) <= self.budget:
+                r = pending.popleft()
+                s = _make_solve(r, self.l_max, self.device)
+                batch.add(s)
+                used += _bytes_estimate(r)
+                live.append([r, s, 0, time.perf_counter() - t0, [], []])
+            if not live:
+                if pending:
+                    raise RuntimeError("a single request exceeds the HBM budget")
+                if i_next < len(reqs):
+                    time.sleep(max(0.0, reqs[i_next].arrival - (time.perf_counter() - t0)))
+                continue
+            peak_live = max(peak_live, len(live))
+            batch.rk4(self.q)
+            still = []
+            for entry in live:
+                r, s = entry[0], entry[1]
+                entry[2] += self.q
+                entry[5].append(self._sample(s))
+                entry[4].append(s.t)
+                if entry[2] >= r.steps:
+                    done = time.perf_counter() - t0
+                    batch.remove(s)
+                    results.append(Result(r.rid, r.arrival, entry[3], done, r.steps, np.array(entry[4]),
+                                          np.array(entry[5])))
+                    used -= _bytes_estimate(r)
+                    s.close()
+                else:
+                    still.append(entry)
+            live = still
+        wall = time.perf_counter() - t0
+        batch.close()
+        out = self._summary(results, wall)
+        out["peak_live"] = peak_live
+        return out
+
+    @staticmethod
+    def _summary(results, wall):
+        lat = np.array([r.latency for r in results])
+        return {"results": sorted(results, key=lambda r: r.rid), "wall_s": wall, "completed": len(results),
+                "solves_per_s": len(results) / wall if wall > 0 else 0.0,
+                "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+                "p99_s": float(np.percentile(lat, 99)) if len(lat) else None}
+
+
+def waveform_error(a, b):
+    """max over requests of the relative L2 difference of two runs' waveforms"""
+    worst = 0.0
+    for ra, rb in zip(a["results"], b["results"]):
+        d = np.linalg.norm(ra.alm - rb.alm)
+        n = np.linalg.norm(rb.alm)
+        worst = max(worst, float(d / n) if n > 0 else float(d))
+    return worst
