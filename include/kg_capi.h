@@ -156,6 +156,12 @@ int kg_diagnostic(kg_solver *h, int index, double *mass_out);
 int kg_set_detectors(kg_solver *h, int n, const double *radii);
 /* detector radii and vertex indices (1-based) */
 int kg_get_detectors(kg_solver *h, double *r_det, int *index_det);
+/* proyector_detectors applied at every vertex shell r(1..Nx) (tools/FFT_sph.f90:247-279
+ * at all radii): alm(l, m, shell) complex, l fastest, m = -L..L, then shell.
+ * precision 0: FP64 reduction per (l, m, shell); 1: the contraction as one GEMM
+ * on the tensor cores (tcgen05), operands split into BF16 head + tail, three
+ * passes hi.hi + hi.lo + lo.hi accumulated in FP32. */
+int kg_project_all_shells(kg_solver *h, int L, int precision, double *host_alm);
 /* sph_harmonics (tools/FFT_sph.f90:282-336) on the vertex grid:
  * Ylm(l, m, j, k) complex, l fastest, m = -L..L, theta then phi */
 int kg_sph_harmonics(kg_solver *h, int L, double *host_ylm);

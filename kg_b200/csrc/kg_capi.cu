@@ -9,6 +9,7 @@
 // kg_boundary.cu and kg_diag.cu.  There is no host fallback: without a usable
 // device kg_create fails with KG_ENODEV.
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -80,6 +81,12 @@ struct kg_solver {
   kg::ShellInterp si;
   const double *normP = nullptr, *cosm = nullptr, *sinm = nullptr, *sint = nullptr;
   std::vector<int> active;
+  // all-shell Y_lm projection (allocated on first use, per L)
+  int ylmL = -1;
+  double* ylm_tab = nullptr;            // normP, cosm, sinm for ylmL
+  unsigned char* ylm_buf = nullptr;     // Ahi, Alo, Bhi, Blo, C, F, alm
+  size_t ylm_bytes = 0;
+  int ylm_b_ready = 0;
   // instrumentation
   long long launches = 0;
   int prof_on = 0;
@@ -121,12 +128,13 @@ size_t field_bytes(const kg_solver* h) { return (size_t)h->g.fs * sizeof(double2
 double2* fld(double2* base, const Grid& g, int v) { return base + (long long)v * g.fs; }
 
 // kernel kinds reported by kg_profile_read: the 13 stage kinds, then these
-enum { PK_GHOST = 13, PK_FACE, PK_RHS, PK_CONVERT, PK_DENSITY, PK_MASS, PK_SHELL, PK_FLUX, PK_PROJECT, PK_COUNT };
+enum { PK_GHOST = 13, PK_FACE, PK_RHS, PK_CONVERT, PK_DENSITY, PK_MASS, PK_SHELL, PK_FLUX, PK_PROJECT,
+       PK_YLM_PREP, PK_YLM_GEMM, PK_YLM_FP64, PK_COUNT };
 const char* const kPkNames[PK_COUNT] = {
     "stage_pirk_s1_psi", "stage_pirk_s1_pi", "stage_pirk2_s2", "stage_pirk3_s2_psi", "stage_pirk3_s2_pi",
     "stage_pirk3_s3", "stage_rk3_1", "stage_rk3_2", "stage_rk3_3", "stage_rk4_1", "stage_rk4_2", "stage_rk4_3",
     "stage_rk4_4", "ghost_fill", "boundary_face", "rhs", "layout_convert", "density", "mass_reduce",
-    "shell_interp", "flux_reduce", "ylm_project"};
+    "shell_interp", "flux_reduce", "ylm_project", "ylm_all_prepare", "ylm_all_gemm_bf16x3", "ylm_all_fp64"};
 
 cudaEvent_t take_event(kg_solver* h) {
   if (!h->pool.empty()) {
@@ -719,7 +727,7 @@ int kg_destroy(kg_solver* h) {
   if (!h) return KG_EINVAL;
   if (h->stream) cudaStreamSynchronize(h->stream);
   void* bufs[] = {h->dmet, h->U, h->S, h->T, h->RK, h->UP, h->HV, h->stage_buf, h->rho, h->partials,
-                  h->d_int, h->d_dbl, h->shells, h->alm, h->flux, h->derr};
+                  h->d_int, h->d_dbl, h->shells, h->alm, h->flux, h->derr, h->ylm_tab, h->ylm_buf};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (auto& row : h->graphs)
@@ -1202,6 +1210,98 @@ int kg_set_detectors(kg_solver* h, int n, const double* radii) {
   if (rc) return rc;
   KG_CK(cudaStreamSynchronize(h->stream));
   return KG_OK;
+}
+
+int kg_project_all_shells(kg_solver* h, int L, int precision, double* host_alm) {
+  if (!h || !host_alm || L < 0 || L > 128 || precision < 0 || precision > 1) return KG_EINVAL;
+  const int Ny = h->Ny, Nz = h->Nz, Nx = h->Nx;
+  const int Nm = (L + 1) * (L + 2) / 2;
+  const int K = Ny * Nz;
+  const int Kp = kg::ylm_gemm_pad_k(K), Mp = kg::ylm_gemm_pad_m(2 * Nx), Np = kg::ylm_gemm_pad_n(2 * Nm);
+  const size_t nalm = (size_t)(L + 1) * (2 * L + 1) * Nx;
+  // buffer plan: Ahi, Alo (Mp x Kp bf16), Bhi, Blo (Np x Kp), C (Mp x Np f32), F (Nx K c128), alm
+  const size_t szA = (size_t)Mp * Kp * 2, szB = (size_t)Np * Kp * 2, szC = (size_t)Mp * Np * 4;
+  const size_t szF = (size_t)Nx * K * 16, szAlm = nalm * 16;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t need = 2 * al(szA) + 2 * al(szB) + al(szC) + al(szF) + al(szAlm);
+  if (h->ylmL != L) {
+    if (h->ylm_tab) cudaFree(h->ylm_tab);
+    h->ylm_tab = nullptr;
+    std::vector<double> tab((size_t)(L + 1) * (L + 1) * Ny + 2 * (size_t)(L + 1) * Nz, 0.0);
+    double* normP = tab.data();
+    double* cosm = normP + (size_t)(L + 1) * (L + 1) * Ny;
+    double* sinm = cosm + (size_t)(L + 1) * Nz;
+    for (int l = 0; l <= L; ++l)
+      for (int m = 0; m <= l; ++m)
+        for (int jv = 1; jv <= Ny; ++jv)
+          normP[((size_t)l * (L + 1) + m) * Ny + jv - 1] = norm_plm(l, m, (double)(jv - 1) * h->dy);
+    for (int m = 0; m <= L; ++m)
+      for (int kv = 1; kv <= Nz; ++kv) {
+        const double ph = (double)(kv - 1) * h->dz;
+        cosm[(size_t)m * Nz + kv - 1] = std::cos(m * ph);
+        sinm[(size_t)m * Nz + kv - 1] = std::sin(m * ph);
+      }
+    int rc = dalloc(h, (void**)&h->ylm_tab, tab.size() * sizeof(double));
+    if (rc) return rc;
+    KG_CK(cudaMemcpyAsync(h->ylm_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    h->ylmL = L;
+    h->ylm_b_ready = 0;
+  }
+  if (h->ylm_bytes < need) {
+    if (h->ylm_buf) cudaFree(h->ylm_buf);
+    h->ylm_buf = nullptr;
+    int rc = dalloc(h, (void**)&h->ylm_buf, need);
+    if (rc) return rc;
+    h->ylm_bytes = need;
+    h->ylm_b_ready = 0;
+  }
+  unsigned char* q = h->ylm_buf;
+  __nv_bfloat16* Ahi = (__nv_bfloat16*)q; q += al(szA);
+  __nv_bfloat16* Alo = (__nv_bfloat16*)q; q += al(szA);
+  __nv_bfloat16* Bhi = (__nv_bfloat16*)q; q += al(szB);
+  __nv_bfloat16* Blo = (__nv_bfloat16*)q; q += al(szB);
+  float* Cm = (float*)q; q += al(szC);
+  double2* F = (double2*)q; q += al(szF);
+  double2* dalm = (double2*)q;
+  const double* normP = h->ylm_tab;
+  const double* cosm = normP + (size_t)(L + 1) * (L + 1) * Ny;
+  const double* sinm = cosm + (size_t)(L + 1) * Nz;
+  const double dydz = h->dy * h->dz;
+  if (precision == 1) {
+    if (!h->ylm_b_ready) {
+      KG_CK(cudaMemsetAsync(Bhi, 0, 2 * al(szB), h->stream));
+      KG_CK(cudaMemsetAsync(Ahi, 0, 2 * al(szA), h->stream));
+      {
+        Prof pf(h, PK_YLM_PREP, 1);
+        kg::launch_ylm_b(L, Ny, Nz, Kp, normP, cosm, sinm, h->sint, Bhi, Blo, h->stream);
+      }
+      h->ylm_b_ready = 1;
+    }
+    {
+      Prof pf(h, PK_YLM_PREP, 1);
+      kg::launch_shells_to_a(h->g, h->U, h->si, Nx, Ny, Nz, Kp, Ahi, Alo, nullptr, h->stream);
+    }
+    {
+      Prof pf(h, PK_YLM_GEMM, 1);
+      if (kg::launch_ylm_gemm(Ahi, Alo, Bhi, Blo, Cm, Mp, Np, Kp, h->derr, h->stream))
+        return set_err(h, KG_ECUDA, "tensor-core projection could not be configured");
+    }
+    {
+      Prof pf(h, PK_YLM_PREP, 1);
+      kg::launch_ylm_assemble(Cm, Np, Nx, L, dydz, dalm, h->stream);
+    }
+  } else {
+    {
+      Prof pf(h, PK_YLM_PREP, 1);
+      kg::launch_shells_to_a(h->g, h->U, h->si, Nx, Ny, Nz, Kp, nullptr, nullptr, F, h->stream);
+    }
+    Prof pf(h, PK_YLM_FP64, 1);
+    kg::launch_ylm_fp64(F, Nx, L, Ny, Nz, normP, cosm, sinm, h->sint, dydz, dalm, h->stream);
+  }
+  KG_CK(cudaGetLastError());
+  KG_CK(cudaMemcpyAsync(host_alm, dalm, szAlm, cudaMemcpyDeviceToHost, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return check_device_flag(h);
 }
 
 int kg_get_detectors(kg_solver* h, double* r_det, int* index_det) {

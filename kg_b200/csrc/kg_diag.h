@@ -29,4 +29,17 @@ void launch_project(const double2* shells, const int* active, int n_det, int L, 
                     const double* cosm, const double* sinm, const double* sint, double dydz, double2* alm,
                     cudaStream_t st);
 
+// all-shell Y_lm projection (kg_ylm_gemm.cu)
+}  // namespace kg
+#include <cuda_bf16.h>
+namespace kg {
+int launch_ylm_gemm(const __nv_bfloat16* Ahi, const __nv_bfloat16* Alo, const __nv_bfloat16* Bhi,
+                    const __nv_bfloat16* Blo, float* C, int Mp, int Np, int Kp, int* err, cudaStream_t st);
+void launch_shells_to_a(const Grid& g, const double2* u, const ShellInterp& si, int Nx, int Ny, int Nz, int Kp,
+                        __nv_bfloat16* Ahi, __nv_bfloat16* Alo, double2* F, cudaStream_t st);
+void launch_ylm_b(int L, int Ny, int Nz, int Kp, const double* normP, const double* cosm, const double* sinm,
+                  const double* sint, __nv_bfloat16* Bhi, __nv_bfloat16* Blo, cudaStream_t st);
+void launch_ylm_assemble(const float* C, int ldc, int Nx, int L, double dydz, double2* alm, cudaStream_t st);
+void launch_ylm_fp64(const double2* F, int Nx, int L, int Ny, int Nz, const double* normP, const double* cosm,
+                     const double* sinm, const double* sint, double dydz, double2* alm, cudaStream_t st);
 }  // namespace kg

@@ -48,6 +48,10 @@ bool tma_available(const Grid& g, const double2* some_state);
 size_t batch_item_bytes();
 int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rsg, int* err, int kchunk, int item0);
 int launch_batch_tma(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks, cudaStream_t st);
+// Y_lm projection over all shells (kg_ylm_gemm.cu)
+int ylm_gemm_pad_m(int rows);
+int ylm_gemm_pad_n(int cols);
+int ylm_gemm_pad_k(int k);
 // batched ghost fill: one launch pair for many solves
 struct GhostDesc {
   Grid g;

@@ -1,0 +1,430 @@
+// kg_ylm_gemm.cu -- the Y_lm projection of phi over every radial shell as a
+// tensor-core GEMM (tcgen05, BF16 inputs, FP32 accumulation in TMEM).
+//
+// The reference projects phi onto Y_lm at a detector radius
+// (tools/FFT_sph.f90:247-279, proyector_detectors in MoL/diagnostic_lib.f90):
+//   a_lm = dtheta dphi sum_jk w_jk f(j,k) conj(Y_lm(j,k)) sin(theta_j)
+// on the vertex sphere, with trapezium weights w_jk.  Over all Nx shells this
+// is one dense contraction.  With f = a + i b, Y_lm = C + i S (m >= 0) and
+// P = a.C', Q = a.S', R = b.C', T = b.S' (C' = w sin C, S' = w sin S):
+//   a_lm = (P + T) + i (R - Q),   a_l,-m = (-1)^m [(P - T) + i (R + Q)].
+// So the projection is the real GEMM  [a; b] (2 Nx x K)  times  [C' S'] (K x 2 Nm)
+// with K = Ny Nz sphere points and Nm = (L+1)(L+2)/2 modes with m >= 0.
+//
+// Precision: each operand is split into a BF16 head and a BF16 tail
+// (x = hi + lo, |lo| <= 2^-8 |x|); the product is formed as the three-term sum
+// hi.hi + hi.lo + lo.hi, all accumulated in FP32 -- three passes of the same
+// BF16 GEMM over K, the dropped lo.lo term being of order 2^-16.
+//
+// GEMM kernel: one CTA per 128 x 256 output tile, 4 warps.  Warp 0 lane 0
+// feeds a 4-deep shared-memory ring with TMA (cp.async.bulk.tensor 2-D,
+// 128-byte swizzle, K-major 64-element slices); warp 1 lane 0 issues
+// tcgen05.mma (kind::f16, M=128, N=256, K=16 per instruction) into a TMEM
+// accumulator of 256 columns and releases ring slots with tcgen05.commit; all
+// four warps then read the accumulator with tcgen05.ld (32 lanes each) and
+// store FP32 rows.  Every mbarrier wait is bounded; a CTA that runs out sets
+// the error flag and still frees its TMEM.  No multicast is used.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "kg_device.cuh"
+#include "kg_internal.h"
+#include "kg_diag.h"
+
+namespace kg {
+namespace {
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+constexpr int A_TILE_B = BM * BK * 2;  // 16 KB
+constexpr int B_TILE_B = BN * BK * 2;  // 32 KB
+constexpr int STAGE_B = A_TILE_B + B_TILE_B;
+constexpr size_t GEMM_SMEM = (size_t)STAGES * STAGE_B + 1024 /*align*/ + 256 /*barriers, tmem slot*/;
+constexpr long long WAIT_LIMIT = 1LL << 24;
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t c) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(c) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(saddr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+  for (long long i = 0; i < WAIT_LIMIT; ++i)
+    if (mbar_try(b, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* tm, int c0, int c1, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(saddr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(saddr(bar))
+      : "memory");
+}
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t smem_addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((smem_addr & 0x3FFFFu) >> 4);  // start address (16-byte units), bits 0-13
+  d |= (uint64_t)1 << 16;                        // leading-byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;              // stride-byte offset between 8-row groups
+  d |= (uint64_t)1 << 46;                        // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                        // layout: 128-byte swizzle
+  return d;
+}
+
+// instruction descriptor: kind::f16 with BF16 A and B, FP32 accumulator, both K-major
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(IDESC), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
+               : "memory");
+}
+
+}  // namespace
+
+// C (M' x ldc, FP32, row-major) = sum over three passes of A_p (M' x K) B_p^T,
+// pass 0: (Ahi, Bhi), 1: (Ahi, Blo), 2: (Alo, Bhi); A and B K-major BF16.
+__global__ void __launch_bounds__(128, 1)
+    ylm_gemm_kernel(const __grid_constant__ CUtensorMap tAhi, const __grid_constant__ CUtensorMap tAlo,
+                    const __grid_constant__ CUtensorMap tBhi, const __grid_constant__ CUtensorMap tBlo, float* C,
+                    int ldc, int Mrows, int Ncols, int K, int* err) {
+  extern __shared__ __align__(1024) unsigned char gsm[];
+  unsigned char* base = gsm + ((1024u - (saddr(gsm) & 1023u)) & 1023u);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)STAGES * STAGE_B);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int nk = K / BK;
+  const int total = 3 * nk;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tmem_slot)),
+                 "r"(BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 32) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  int bad = 0;
+
+  if (warp == 0 && lane == 0) {
+    // producer
+    for (int it = 0; it < total && !bad; ++it) {
+      const int s = it % STAGES;
+      if (it >= STAGES && !mbar_wait(&empty[s], ((it / STAGES) - 1) & 1)) {
+        bad = 1;
+        break;
+      }
+      const int pass = it / nk, kb = it % nk;
+      unsigned char* sa = base + (size_t)s * STAGE_B;
+      unsigned char* sb = sa + A_TILE_B;
+      mbar_expect_tx(&full[s], STAGE_B);
+      tma_2d(sa, pass == 2 ? &tAlo : &tAhi, kb * BK, m0, &full[s]);
+      tma_2d(sb, pass == 1 ? &tBlo : &tBhi, kb * BK, n0, &full[s]);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    for (int it = 0; it < total && !bad; ++it) {
+      const int s = it % STAGES;
+      if (!mbar_wait(&full[s], (it / STAGES) & 1)) {
+        bad = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t sa = saddr(base + (size_t)s * STAGE_B);
+      const uint32_t sb = sa + A_TILE_B;
+#pragma unroll
+      for (int k = 0; k < BK / 16; ++k)
+        umma(tmem, sw128_desc(sa + k * 32), sw128_desc(sb + k * 32), (it > 0 || k > 0) ? 1u : 0u);
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);
+  }
+  __syncwarp();
+  // epilogue: every warp reads its 32 accumulator lanes (tcgen05.ld is warp-collective,
+  // so the error decision is made block-uniform first)
+  if (!mbar_wait(done, 0)) bad = 1;
+  bad = __syncthreads_or(bad);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const int row = m0 + warp * 32 + lane;
+  if (!bad) {
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      uint32_t v[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+            "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+            "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < Mrows && n0 + c0 < Ncols) {
+        float4* dst = reinterpret_cast<float4*>(C + (size_t)row * ldc + n0 + c0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                               __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+      }
+    }
+  }
+  if (bad && threadIdx.x == 0) atomicExch(err, 2);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// operand preparation
+
+// phi on every vertex shell (domain_to_sph at all r), split into BF16 head/tail:
+// A rows 0..Nx-1 = Re, Nx..2Nx-1 = Im, columns (jv, kv) -> jv + Ny kv, row pitch Kp
+__global__ void shells_to_a_kernel(Grid g, const double2* __restrict__ u, ShellInterp si, int Nx, int Ny, int Nz,
+                                   int Kp, __nv_bfloat16* Ahi, __nv_bfloat16* Alo, double2* Fout) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)Nx * Ny * Nz;
+  if (t >= n) return;
+  const int jv = (int)(t % Ny);
+  const long long r2 = t / Ny;
+  const int kv = (int)(r2 % Nz);
+  const int iv = (int)(r2 / Nz);  // 0-based shell: vertex r index iv+1 -> evolution ii = iv
+  const int ir = iv, ith = si.i_th[jv], iph = si.i_ph[kv];
+  double2 f;
+  const int fl = si.th_flag[jv];
+  if (fl == 1) f = u[off3(g, ir, 0, iph)];
+  else if (fl == 2) f = u[off3(g, ir, g.NJ - 1, iph)];
+  else {
+    const double wt = si.w_th[jv], wp = si.w_ph[kv];
+    const int ip1 = iph + 1;
+    const double2 f00 = cadd(rmul(1.0 - wp, u[off3(g, ir, ith, iph)]), rmul(wp, u[off3(g, ir, ith, ip1)]));
+    const double2 f01 = cadd(rmul(1.0 - wp, u[off3(g, ir, ith + 1, iph)]), rmul(wp, u[off3(g, ir, ith + 1, ip1)]));
+    f = cadd(rmul(1.0 - wt, f00), rmul(wt, f01));
+  }
+  const long long col = jv + (long long)Ny * kv;
+  if (Fout) Fout[(long long)iv * Ny * Nz + col] = f;
+  if (Ahi) {
+    const float re = (float)f.x, im = (float)f.y;
+    const __nv_bfloat16 rh = __float2bfloat16_rn(re), ih = __float2bfloat16_rn(im);
+    Ahi[(long long)iv * Kp + col] = rh;
+    Alo[(long long)iv * Kp + col] = __float2bfloat16_rn(re - __bfloat162float(rh));
+    Ahi[(long long)(Nx + iv) * Kp + col] = ih;
+    Alo[(long long)(Nx + iv) * Kp + col] = __float2bfloat16_rn(im - __bfloat162float(ih));
+  }
+}
+
+// B^T rows: n < Nm: w sin C_lm, Nm <= n < 2Nm: w sin S_lm (mode index n of (l, m>=0) as l(l+1)/2 + m)
+__global__ void ylm_b_kernel(int L, int Ny, int Nz, int Kp, const double* __restrict__ normP,
+                             const double* __restrict__ cosm, const double* __restrict__ sinm,
+                             const double* __restrict__ sint, __nv_bfloat16* Bhi, __nv_bfloat16* Blo) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int Nm = (L + 1) * (L + 2) / 2;
+  const long long n = (long long)2 * Nm * Ny * Nz;
+  if (t >= n) return;
+  const int jv = (int)(t % Ny);
+  const long long r2 = t / Ny;
+  const int kv = (int)(r2 % Nz);
+  const int row = (int)(r2 / Nz);
+  const int mode = row % Nm, part = row / Nm;
+  int l = 0;
+  while ((l + 1) * (l + 2) / 2 <= mode) ++l;
+  const int m = mode - l * (l + 1) / 2;
+  const int sel = ((jv == 0 || jv == Ny - 1) ? 1 : 0) + 2 * ((kv == 0 || kv == Nz - 1) ? 1 : 0);
+  const double w = sel == 0 ? 1.0 : (sel == 3 ? 0.25 : 0.5);
+  const double np = normP[((long long)l * (L + 1) + m) * Ny + jv];
+  const double trig = part == 0 ? cosm[(long long)m * Nz + kv] : sinm[(long long)m * Nz + kv];
+  const float v = (float)(w * sint[jv] * (np * trig));
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  const long long o = (long long)row * Kp + jv + (long long)Ny * kv;
+  Bhi[o] = h;
+  Blo[o] = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+// a_lm(l, m, shell) from the GEMM blocks P Q / R T
+__global__ void ylm_assemble_kernel(const float* __restrict__ C, int ldc, int Nx, int L, double dydz,
+                                    double2* __restrict__ alm) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int NL = L + 1, NM = 2 * L + 1;
+  const long long n = (long long)NL * NM * Nx;
+  if (t >= n) return;
+  const int l = (int)(t % NL);
+  const int mi = (int)((t / NL) % NM);
+  const int iv = (int)(t / ((long long)NL * NM));
+  const int m = mi - L;
+  double2 out = c2(0.0, 0.0);
+  if (m >= -l && m <= l) {
+    const int am = m < 0 ? -m : m;
+    const int Nm = (L + 1) * (L + 2) / 2;
+    const int mode = l * (l + 1) / 2 + am;
+    const double P = C[(size_t)iv * ldc + mode], Q = C[(size_t)iv * ldc + Nm + mode];
+    const double R = C[(size_t)(Nx + iv) * ldc + mode], T = C[(size_t)(Nx + iv) * ldc + Nm + mode];
+    if (m >= 0) out = c2(P + T, R - Q);
+    else {
+      const double sg = (am & 1) ? -1.0 : 1.0;
+      out = c2(sg * (P - T), sg * (R + Q));
+    }
+    out = rmul(dydz, out);
+  }
+  alm[t] = out;
+}
+
+// FP64 reference projection over all shells: one block per (l, m, shell)
+__global__ void ylm_fp64_kernel(const double2* __restrict__ F, int Nx, int L, int Ny, int Nz,
+                                const double* __restrict__ normP, const double* __restrict__ cosm,
+                                const double* __restrict__ sinm, const double* __restrict__ sint, double dydz,
+                                double2* alm) {
+  const int l = blockIdx.x, mi = blockIdx.y, iv = blockIdx.z;
+  const int m = mi - L;
+  const long long o = (long long)l + (L + 1) * ((long long)mi + (2 * L + 1) * iv);
+  if (m < -l || m > l) {
+    if (threadIdx.x == 0) alm[o] = c2(0.0, 0.0);
+    return;
+  }
+  const int am = m < 0 ? -m : m;
+  const double sgn = (am & 1) ? -1.0 : 1.0;
+  const double* P = normP + ((long long)l * (L + 1) + am) * Ny;
+  const double* cm = cosm + (long long)am * Nz;
+  const double* sm = sinm + (long long)am * Nz;
+  const double2* f = F + (long long)iv * Ny * Nz;
+  double ax = 0.0, ay = 0.0;
+  for (int t = threadIdx.x; t < Ny * Nz; t += blockDim.x) {
+    const int jv = t % Ny, kv = t / Ny;
+    const double np = P[jv];
+    double yx = np * cm[kv], yy = np * sm[kv];
+    if (m < 0) { yx = sgn * yx; yy = sgn * -yy; }
+    const double2 a = f[t];
+    const double fyx = a.x * yx - a.y * -yy, fyy = a.x * -yy + a.y * yx;
+    const double s = sint[jv];
+    const int sel = ((jv == 0 || jv == Ny - 1) ? 1 : 0) + 2 * ((kv == 0 || kv == Nz - 1) ? 1 : 0);
+    const double w = sel == 0 ? 1.0 : (sel == 3 ? 0.25 : 0.5);
+    ax += w * (fyx * s);
+    ay += w * (fyy * s);
+  }
+  __shared__ double sx[32], sy[32];
+  for (int off = 16; off > 0; off >>= 1) {
+    ax += __shfl_down_sync(0xffffffffu, ax, off);
+    ay += __shfl_down_sync(0xffffffffu, ay, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sx[threadIdx.x >> 5] = ax;
+    sy[threadIdx.x >> 5] = ay;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double bx = 0.0, by = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      bx += sx[w];
+      by += sy[w];
+    }
+    alm[o] = c2(dydz * bx, dydz * by);
+  }
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                             const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                             CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeFn enc() {
+  static EncodeFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeFn)p;
+  }
+  return fn;
+}
+bool map_kmajor(CUtensorMap* tm, const __nv_bfloat16* p, int Kp, int rows, int box_rows) {
+  EncodeFn fn = enc();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
+  cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)p, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+}  // namespace
+
+int ylm_gemm_pad_m(int rows) { return (rows + BM - 1) / BM * BM; }
+int ylm_gemm_pad_n(int cols) { return (cols + BN - 1) / BN * BN; }
+int ylm_gemm_pad_k(int k) { return (k + BK - 1) / BK * BK; }
+
+// C (Mp x Np) = three-pass split-BF16 product; all dimensions already padded
+int launch_ylm_gemm(const __nv_bfloat16* Ahi, const __nv_bfloat16* Alo, const __nv_bfloat16* Bhi,
+                    const __nv_bfloat16* Blo, float* C, int Mp, int Np, int Kp, int* err, cudaStream_t st) {
+  CUtensorMap a0, a1, b0, b1;
+  if (!map_kmajor(&a0, Ahi, Kp, Mp, BM) || !map_kmajor(&a1, Alo, Kp, Mp, BM) || !map_kmajor(&b0, Bhi, Kp, Np, BN) ||
+      !map_kmajor(&b1, Blo, Kp, Np, BN))
+    return -1;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(ylm_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM) !=
+        cudaSuccess)
+      return -1;
+    attr = true;
+  }
+  ylm_gemm_kernel<<<dim3(Np / BN, Mp / BM), 128, GEMM_SMEM, st>>>(a0, a1, b0, b1, C, Np, Mp, Np, Kp, err);
+  return 0;
+}
+
+void launch_shells_to_a(const Grid& g, const double2* u, const ShellInterp& si, int Nx, int Ny, int Nz, int Kp,
+                        __nv_bfloat16* Ahi, __nv_bfloat16* Alo, double2* F, cudaStream_t st) {
+  const long long n = (long long)Nx * Ny * Nz;
+  shells_to_a_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, u, si, Nx, Ny, Nz, Kp, Ahi, Alo, F);
+}
+
+void launch_ylm_b(int L, int Ny, int Nz, int Kp, const double* normP, const double* cosm, const double* sinm,
+                  const double* sint, __nv_bfloat16* Bhi, __nv_bfloat16* Blo, cudaStream_t st) {
+  const int Nm = (L + 1) * (L + 2) / 2;
+  const long long n = (long long)2 * Nm * Ny * Nz;
+  ylm_b_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(L, Ny, Nz, Kp, normP, cosm, sinm, sint, Bhi, Blo);
+}
+
+void launch_ylm_assemble(const float* C, int ldc, int Nx, int L, double dydz, double2* alm, cudaStream_t st) {
+  const long long n = (long long)(L + 1) * (2 * L + 1) * Nx;
+  ylm_assemble_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(C, ldc, Nx, L, dydz, alm);
+}
+
+void launch_ylm_fp64(const double2* F, int Nx, int L, int Ny, int Nz, const double* normP, const double* cosm,
+                     const double* sinm, const double* sint, double dydz, double2* alm, cudaStream_t st) {
+  ylm_fp64_kernel<<<dim3(L + 1, 2 * L + 1, Nx), 256, 0, st>>>(F, Nx, L, Ny, Nz, normP, cosm, sinm, sint, dydz, alm);
+}
+
+}  // namespace kg

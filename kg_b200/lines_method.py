@@ -250,6 +250,13 @@ class ScalarField(LinesMethod):
         self.momentum = np.zeros((self.n_det, 3))
         self.alm = np.zeros((self.n_det, 2 * self.l_max + 1, self.l_max + 1), np.complex128)
 
+    def project_all_shells(self, L, precision=1):
+        """a_lm (l <= L) of phi on every vertex shell: array (Nx, 2L+1, L+1) complex.
+        precision 1: split-BF16 tensor-core GEMM (FP32 accumulation); 0: FP64."""
+        out = np.zeros((self.Nx, 2 * L + 1, L + 1), np.complex128)
+        self._ck(self._lib.kg_project_all_shells(self._h, L, precision, _dp(out.view(np.float64))))
+        return out
+
     def detectors(self):
         r = np.zeros(self.n_det)
         idx = np.zeros(self.n_det, np.int32)

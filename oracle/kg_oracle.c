@@ -895,6 +895,21 @@ void kgo_proyector_detectors(const kgo *s, int L, double *alm) {
   free(sl); free(ylm);
 }
 
+/* project_sh at every vertex shell iv = 1..Nx (tools/FFT_sph.f90:247-279 with
+ * domain_to_sph at r = rv(iv), tools/FFT_sph.f90:525-651): alm(l, m, shell). */
+void kgo_project_all_shells(const kgo *s, int L, double *alm) {
+  size_t ny = s->Ny, nz = s->Nz;
+  double *ylm = xcalloc(2 * (size_t)(L + 1) * (2 * L + 1) * ny * nz, sizeof(double));
+  kgo_sph_harmonics(s, L, ylm);
+  cplx *sl = xcalloc(ny * nz, sizeof(cplx));
+  const size_t per = (size_t)(L + 1) * (2 * L + 1);
+  for (int iv = 1; iv <= s->Nx; ++iv) {
+    kgo_domain_to_sph_shell(s, s->u[0], iv, sl);
+    kgo_project_sh(s, sl, ylm, L, alm + 2 * per * (size_t)(iv - 1));
+  }
+  free(sl); free(ylm);
+}
+
 /* ------------------------------------------------------------------ */
 /* construction and state access                                       */
 

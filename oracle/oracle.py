@@ -65,6 +65,7 @@ def lib():
         L.kgo_integrate_real.restype = C.c_double
         L.kgo_currents_detectors.argtypes = [P, D]
         L.kgo_proyector_detectors.argtypes = [P, I, D]
+        L.kgo_project_all_shells.argtypes = [P, I, D]
         L.kgo_sph_harmonics.argtypes = [P, I, D]
         L.kgo_project_sh.argtypes = [P, D, D, I, D]
         L.kgo_domain_to_sph_shell.argtypes = [P, D, I, D]
@@ -201,6 +202,12 @@ class Oracle:
     def proyector_detectors(self, L):
         out = np.zeros((self.n_det, 2 * L + 1, L + 1), np.complex128)
         lib().kgo_proyector_detectors(self.h, L, _dp(out.view(np.float64)))
+        return out
+
+    def project_all_shells(self, L):
+        """a_lm on every vertex shell: (Nx, 2L+1, L+1) complex"""
+        out = np.zeros((self.Nx, 2 * L + 1, L + 1), np.complex128)
+        lib().kgo_project_all_shells(self.h, L, _dp(out.view(np.float64)))
         return out
 
     def sph_harmonics(self, L):

@@ -233,3 +233,17 @@ def test_detectors_and_mass():
     o.set_state(_ic())
     m = o.mass()
     assert np.isfinite(m) and m > 0
+
+
+def test_all_shell_projection_contains_detector_projection():
+    """project_all_shells at shell index_det is proyector_detectors at that detector"""
+    g = GRID
+    o = Oracle(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], m=0.3, n_det=5)
+    o.set_state(_ic())
+    _, idx = o.detectors()
+    a_det = o.proyector_detectors(6)
+    a_all = o.project_all_shells(6)
+    assert a_all.shape == (g["Nx"], 13, 7)
+    for d, iv in enumerate(idx):
+        if iv > 0:
+            assert np.array_equal(a_det[d], a_all[iv - 1])
