@@ -181,6 +181,71 @@ def serve_leg(count, device):
     return out
 
 
+def projection_leg(mol, lib, h, L=64, reps=3):
+    """All-shell Y_lm projection to l <= L over every radial shell of the solve's
+    current state (the precision form's diagnostic): the split-BF16 tcgen05 GEMM
+    [2 Nx x K] . [K x 2 Nm] (K = Ny Nz sphere points, Nm = (L+1)(L+2)/2 modes
+    with m >= 0) timed per kernel with CUDA events, and its error against the
+    FP64 projection of the same state."""
+    Nx, Ny, Nz = mol.Nx, mol.Ny, mol.Nz
+    K = Ny * Nz
+    Nm = (L + 1) * (L + 2) // 2
+    pad = lambda v, b: (v + b - 1) // b * b
+    Mp, Np, Kp = pad(2 * Nx, 128), pad(2 * Nm, 256), pad(K, 64)
+    nk = lib.kg_profile_kinds()
+    names = [lib.kg_profile_kind_name(i).decode() for i in range(nk)]
+    ms = (C.c_double * nk)()
+    cnt = (C.c_longlong * nk)()
+
+    def timed(precision, n):
+        out = np.zeros((Nx, 2 * L + 1, L + 1), np.complex128)
+        lib.kg_profile_read(h, ms, cnt)
+        lib.kg_profile_enable(h, 1)
+        for _ in range(n):
+            mol._ck(lib.kg_project_all_shells(h, L, precision, out.ctypes.data_as(C.POINTER(C.c_double))))
+        lib.kg_profile_read(h, ms, cnt)
+        lib.kg_profile_enable(h, 0)
+        return out, {names[i]: (ms[i], cnt[i]) for i in range(nk) if cnt[i] > 0}
+
+    timed(1, 1)  # tables, B operand, tensor maps
+    a_t, kt = timed(1, reps)
+    a_64, k64 = timed(0, 1)
+    g_ms, g_n = kt["ylm_all_gemm_bf16x3"]
+    p_ms, p_n = kt.get("ylm_all_prepare", (0.0, 1))
+    f_ms, _ = k64["ylm_all_fp64"]
+    issued = 3 * 2.0 * Mp * Np * Kp
+    useful = 2.0 * (2 * Nx) * K * (2 * Nm)
+    complex_equiv = 8.0 * Nx * K * (L + 1) ** 2
+    gemm_s = g_ms / g_n / 1e3
+    d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = float(d.get("bf16_tflops", 1590.0))
+    diff = a_t - a_64
+    shell_err = np.sqrt(np.sum(np.abs(diff) ** 2, axis=(1, 2)))
+    shell_norm = np.sqrt(np.sum(np.abs(a_64) ** 2, axis=(1, 2)))
+    # shells where the field is below 1e-6 of its peak shell (the Gaussian tail, down
+    # to values FP32 cannot hold) are left out of the per-shell ratios
+    live = shell_norm > 1e-6 * shell_norm.max()
+    coef_err = np.abs(diff).reshape(Nx, -1).max(axis=1)
+    return {
+        "workload": f"a_lm for l<={L} on all {Nx} vertex shells of the {Ny}x{Nz} sphere (K={K}), "
+                    f"GEMM [{2 * Nx}x{K}].[{K}x{2 * Nm}] padded to {Mp}x{Kp}x{Np}, split-BF16 3 passes",
+        "gemm_ms": g_ms / g_n, "prepare_ms_per_call": p_ms / reps, "fp64_ms": f_ms,
+        "tensor_roofline": {"bound": "tensor", "achieved": issued / gemm_s / 1e12, "peak": peak,
+                            "unit": "TFLOP/s", "frac": issued / gemm_s / 1e12 / peak,
+                            "peak_source": "measured bf16 burst" if d else "fallback",
+                            "issued_flop_per_launch": issued},
+        "useful_real_tflops": useful / gemm_s / 1e12,
+        "complex_equiv_tflops": complex_equiv / gemm_s / 1e12,
+        "speedup_vs_fp64_projection": f_ms / (g_ms / g_n + p_ms / reps),
+        "energy_norm_rel_err_vs_fp64": float(np.linalg.norm(diff) / np.linalg.norm(a_64)),
+        "max_shell_energy_rel_err": float((shell_err[live] / shell_norm[live]).max()) if live.any() else None,
+        "max_coef_err_over_shell_norm": float((coef_err[live] / shell_norm[live]).max()) if live.any() else None,
+        "error_note": "each coefficient carries an absolute error ~2^-17 of its shell's norm (BF16 split); the "
+                      "energy-norm error sums it over all (L+1)^2 modes while the field's energy sits in l<=4",
+    }
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -227,6 +292,7 @@ def main():
     ap.add_argument("--variant", type=int, default=None, help="stage-kernel form (kg_set_kernel_variant)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--serve-count", type=int, default=120)
+    ap.add_argument("--no-projection", action="store_true", help="skip the all-shell Y_lm projection leg")
     args = ap.parse_args()
     if args.grid:
         nx, ny, nz = (int(v) for v in args.grid.split(","))
@@ -366,6 +432,8 @@ def main():
                 "value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": (state_bytes + 8 * args.steps) / args.steps},
             "gpu_launches": int(launches), "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_projection:
+        line["projection"] = projection_leg(mol, lib, h)
     if rank == 0 and world == 1 and not args.no_serve and not args.grid:
         mol.close()
         line["serving"] = serve_leg(args.serve_count, local)

@@ -498,8 +498,11 @@ int build_detectors(kg_solver* h, const double* radii = nullptr) {
   hd.insert(hd.end(), normP.begin(), normP.end());
   hd.insert(hd.end(), cosm.begin(), cosm.end());
   hd.insert(hd.end(), sinm.begin(), sinm.end());
-  KG_CK(cudaMemcpy(h->d_int, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice));
-  KG_CK(cudaMemcpy(h->d_dbl, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // on the solver's stream, behind dalloc's zero fill of the same buffers (the
+  // stream is non-blocking, so a legacy-stream copy could land before that fill)
+  KG_CK(cudaMemcpyAsync(h->d_int, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  KG_CK(cudaMemcpyAsync(h->d_dbl, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
   const int* ip = h->d_int;
   h->si.active = ip;
   h->si.i_r = ip + n;
@@ -1517,7 +1520,8 @@ int kg_batch_create(int device, kg_batch** out) {
   b->blocks = 2 * sms;
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess ||
-      cudaMalloc((void**)&b->derr, 16) != cudaSuccess || cudaMemset(b->derr, 0, 16) != cudaSuccess) {
+      cudaMalloc((void**)&b->derr, 16) != cudaSuccess || cudaMemsetAsync(b->derr, 0, 16, b->stream) != cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess) {
     kg_batch_destroy(b);
     return KG_ECUDA;
   }
@@ -1633,7 +1637,8 @@ int kg_batch_synchronize(kg_batch* b) {
   if (!b) return KG_EINVAL;
   KG_BCK(cudaStreamSynchronize(b->stream));
   int f = 0;
-  KG_BCK(cudaMemcpy(&f, b->derr, sizeof(int), cudaMemcpyDeviceToHost));
+  KG_BCK(cudaMemcpyAsync(&f, b->derr, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  KG_BCK(cudaStreamSynchronize(b->stream));
   if (f) {
     b->err = "a device wait ran out in a batched launch";
     return KG_ETIMEOUT;

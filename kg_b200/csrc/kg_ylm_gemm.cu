@@ -301,55 +301,77 @@ __global__ void ylm_assemble_kernel(const float* __restrict__ C, int ldc, int Nx
   alm[t] = out;
 }
 
-// FP64 reference projection over all shells: one block per (l, m, shell)
-__global__ void ylm_fp64_kernel(const double2* __restrict__ F, int Nx, int L, int Ny, int Nz,
-                                const double* __restrict__ normP, const double* __restrict__ cosm,
-                                const double* __restrict__ sinm, const double* __restrict__ sint, double dydz,
-                                double2* alm) {
-  const int l = blockIdx.x, mi = blockIdx.y, iv = blockIdx.z;
-  const int m = mi - L;
-  const long long o = (long long)l + (L + 1) * ((long long)mi + (2 * L + 1) * iv);
-  if (m < -l || m > l) {
-    if (threadIdx.x == 0) alm[o] = c2(0.0, 0.0);
-    return;
-  }
-  const int am = m < 0 ? -m : m;
-  const double sgn = (am & 1) ? -1.0 : 1.0;
-  const double* P = normP + ((long long)l * (L + 1) + am) * Ny;
-  const double* cm = cosm + (long long)am * Nz;
-  const double* sm = sinm + (long long)am * Nz;
+// FP64 projection over all shells.  One block per (l-chunk, m >= 0, shell): the
+// shell is read once for LC degrees and both signs of m, from four real sums per
+// degree (f = a + ib, Y_lm = C + iS, m >= 0):
+//   a_lm   = dtdp sum w sin [(aC + bS) + i (bC - aS)]
+//   a_l,-m = (-1)^m dtdp sum w sin [(aC - bS) + i (bC + aS)]
+constexpr int LC = 8;
+__global__ void __launch_bounds__(256) ylm_fp64_kernel(const double2* __restrict__ F, int Nx, int L, int Ny, int Nz,
+                                                       const double* __restrict__ normP,
+                                                       const double* __restrict__ cosm,
+                                                       const double* __restrict__ sinm,
+                                                       const double* __restrict__ sint, double dydz,
+                                                       double2* __restrict__ alm) {
+  const int l0 = blockIdx.x * LC, m = blockIdx.y, iv = blockIdx.z;
+  const int NL = L + 1, NM = 2 * L + 1;
+  double acc[LC][4];
+#pragma unroll
+  for (int q = 0; q < LC; ++q) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.0;
   const double2* f = F + (long long)iv * Ny * Nz;
-  double ax = 0.0, ay = 0.0;
+  const double* cm = cosm + (long long)m * Nz;
+  const double* sm = sinm + (long long)m * Nz;
   for (int t = threadIdx.x; t < Ny * Nz; t += blockDim.x) {
     const int jv = t % Ny, kv = t / Ny;
-    const double np = P[jv];
-    double yx = np * cm[kv], yy = np * sm[kv];
-    if (m < 0) { yx = sgn * yx; yy = sgn * -yy; }
-    const double2 a = f[t];
-    const double fyx = a.x * yx - a.y * -yy, fyy = a.x * -yy + a.y * yx;
-    const double s = sint[jv];
     const int sel = ((jv == 0 || jv == Ny - 1) ? 1 : 0) + 2 * ((kv == 0 || kv == Nz - 1) ? 1 : 0);
-    const double w = sel == 0 ? 1.0 : (sel == 3 ? 0.25 : 0.5);
-    ax += w * (fyx * s);
-    ay += w * (fyy * s);
-  }
-  __shared__ double sx[32], sy[32];
-  for (int off = 16; off > 0; off >>= 1) {
-    ax += __shfl_down_sync(0xffffffffu, ax, off);
-    ay += __shfl_down_sync(0xffffffffu, ay, off);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    sx[threadIdx.x >> 5] = ax;
-    sy[threadIdx.x >> 5] = ay;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double bx = 0.0, by = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      bx += sx[w];
-      by += sy[w];
+    const double w = (sel == 0 ? 1.0 : (sel == 3 ? 0.25 : 0.5)) * sint[jv];
+    const double2 a = f[t];
+    const double c = cm[kv], s = sm[kv];
+    const double ac = w * (a.x * c), bs = w * (a.y * s), bc = w * (a.y * c), as = w * (a.x * s);
+#pragma unroll
+    for (int q = 0; q < LC; ++q) {
+      const int l = l0 + q;
+      if (l <= L && l >= m) {
+        const double np = normP[((long long)l * NL + m) * Ny + jv];
+        acc[q][0] += np * ac;
+        acc[q][1] += np * bs;
+        acc[q][2] += np * bc;
+        acc[q][3] += np * as;
+      }
     }
-    alm[o] = c2(dydz * bx, dydz * by);
+  }
+  __shared__ double red[8][LC * 4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < LC; ++q)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      double v = acc[q][e];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if (lane == 0) red[warp][q * 4 + e] = v;
+    }
+  __syncthreads();
+  if (threadIdx.x < LC) {
+    const int q = threadIdx.x, l = l0 + q;
+    if (l > L) return;
+    double ac = 0.0, bs = 0.0, bc = 0.0, as = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      ac += red[w][q * 4 + 0];
+      bs += red[w][q * 4 + 1];
+      bc += red[w][q * 4 + 2];
+      as += red[w][q * 4 + 3];
+    }
+    double2* o = alm + (long long)NL * NM * iv;
+    if (l < m) {  // outside |m| <= l: zero both entries
+      o[l + NL * (m + L)] = c2(0.0, 0.0);
+      o[l + NL * (-m + L)] = c2(0.0, 0.0);
+      return;
+    }
+    o[l + NL * (m + L)] = c2(dydz * (ac + bs), dydz * (bc - as));
+    if (m > 0) {
+      const double sg = (m & 1) ? -1.0 : 1.0;
+      o[l + NL * (-m + L)] = c2(dydz * (sg * (ac - bs)), dydz * (sg * (bc + as)));
+    }
   }
 }
 
@@ -424,7 +446,8 @@ void launch_ylm_assemble(const float* C, int ldc, int Nx, int L, double dydz, do
 
 void launch_ylm_fp64(const double2* F, int Nx, int L, int Ny, int Nz, const double* normP, const double* cosm,
                      const double* sinm, const double* sint, double dydz, double2* alm, cudaStream_t st) {
-  ylm_fp64_kernel<<<dim3(L + 1, 2 * L + 1, Nx), 256, 0, st>>>(F, Nx, L, Ny, Nz, normP, cosm, sinm, sint, dydz, alm);
+  ylm_fp64_kernel<<<dim3((L + LC) / LC, L + 1, Nx), 256, 0, st>>>(F, Nx, L, Ny, Nz, normP, cosm, sinm, sint, dydz,
+                                                                   alm);
 }
 
 }  // namespace kg
