@@ -162,6 +162,14 @@ int kg_get_detectors(kg_solver *h, double *r_det, int *index_det);
  * on the tensor cores (tcgen05), operands split into BF16 head + tail, three
  * passes hi.hi + hi.lo + lo.hi accumulated in FP32. */
 int kg_project_all_shells(kg_solver *h, int L, int precision, double *host_alm);
+/* generate_full_bessel_basis (tools/FFT_sph.f90:13-95): k_values(0:L, Nk) and the
+ * normalised j_basis(0:L, Nk, Nx) on the vertex radii, Fortran order (l fastest);
+ * either output may be NULL.  k_ln = (n-th zero of j_l) / r_max. */
+int kg_bessel_basis(kg_solver *h, int L, int Nk, double *k_values, double *j_basis);
+/* SphFT_discrete_radial (tools/FFT_sph.f90:213-244): ft(1:Nk, 0:L, -L:L) complex,
+ * n fastest, = trapezium over the shells of flm(r) j_basis(l,n,r) r^2, with flm
+ * the all-shell projection of phi (precision as kg_project_all_shells). */
+int kg_sph_ft_radial(kg_solver *h, int L, int Nk, int precision, double *host_ft);
 /* sph_harmonics (tools/FFT_sph.f90:282-336) on the vertex grid:
  * Ylm(l, m, j, k) complex, l fastest, m = -L..L, theta then phi */
 int kg_sph_harmonics(kg_solver *h, int L, double *host_ylm);

@@ -76,6 +76,8 @@ SIGNATURES = [
     ("kg_set_detectors", _I, [_P, _I, _D]),
     ("kg_sph_harmonics", _I, [_P, _I, _D]),
     ("kg_project_all_shells", _I, [_P, _I, _I, _D]),
+    ("kg_bessel_basis", _I, [_P, _I, _I, _D, _D]),
+    ("kg_sph_ft_radial", _I, [_P, _I, _I, _I, _D]),
     ("kg_profile_enable", _I, [_P, _I]),
     ("kg_profile_read", _I, [_P, _D, C.POINTER(C.c_longlong)]),
     ("kg_profile_kinds", _I, []),

@@ -87,6 +87,11 @@ struct kg_solver {
   unsigned char* ylm_buf = nullptr;     // Ahi, Alo, Bhi, Blo, C, F, alm
   size_t ylm_bytes = 0;
   int ylm_b_ready = 0;
+  // spherical-Bessel radial basis (per L, Nk) and transform output
+  int radL = -1, radNk = -1;
+  std::vector<double> rad_k, rad_basis;  // k[l*Nk+n], basis[(l*Nk+n)*Nx+i]
+  double* rad_jr = nullptr;              // device: j_basis * r^2, [(l*Nx+i)*Nk+n]
+  double2* rad_ft = nullptr;             // device: ft(Nk, 0:L, -L:L)
   // instrumentation
   long long launches = 0;
   int prof_on = 0;
@@ -129,12 +134,12 @@ double2* fld(double2* base, const Grid& g, int v) { return base + (long long)v *
 
 // kernel kinds reported by kg_profile_read: the 13 stage kinds, then these
 enum { PK_GHOST = 13, PK_FACE, PK_RHS, PK_CONVERT, PK_DENSITY, PK_MASS, PK_SHELL, PK_FLUX, PK_PROJECT,
-       PK_YLM_PREP, PK_YLM_GEMM, PK_YLM_FP64, PK_COUNT };
+       PK_YLM_PREP, PK_YLM_GEMM, PK_YLM_FP64, PK_RADIAL, PK_COUNT };
 const char* const kPkNames[PK_COUNT] = {
     "stage_pirk_s1_psi", "stage_pirk_s1_pi", "stage_pirk2_s2", "stage_pirk3_s2_psi", "stage_pirk3_s2_pi",
     "stage_pirk3_s3", "stage_rk3_1", "stage_rk3_2", "stage_rk3_3", "stage_rk4_1", "stage_rk4_2", "stage_rk4_3",
     "stage_rk4_4", "ghost_fill", "boundary_face", "rhs", "layout_convert", "density", "mass_reduce",
-    "shell_interp", "flux_reduce", "ylm_project", "ylm_all_prepare", "ylm_all_gemm_bf16x3", "ylm_all_fp64"};
+    "shell_interp", "flux_reduce", "ylm_project", "ylm_all_prepare", "ylm_all_gemm_bf16x3", "ylm_all_fp64", "radial_ft"};
 
 cudaEvent_t take_event(kg_solver* h) {
   if (!h->pool.empty()) {
@@ -730,7 +735,8 @@ int kg_destroy(kg_solver* h) {
   if (!h) return KG_EINVAL;
   if (h->stream) cudaStreamSynchronize(h->stream);
   void* bufs[] = {h->dmet, h->U, h->S, h->T, h->RK, h->UP, h->HV, h->stage_buf, h->rho, h->partials,
-                  h->d_int, h->d_dbl, h->shells, h->alm, h->flux, h->derr, h->ylm_tab, h->ylm_buf};
+                  h->d_int, h->d_dbl, h->shells, h->alm, h->flux, h->derr, h->ylm_tab, h->ylm_buf,
+                  h->rad_jr, h->rad_ft};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (auto& row : h->graphs)
@@ -1215,8 +1221,11 @@ int kg_set_detectors(kg_solver* h, int n, const double* radii) {
   return KG_OK;
 }
 
-int kg_project_all_shells(kg_solver* h, int L, int precision, double* host_alm) {
-  if (!h || !host_alm || L < 0 || L > 128 || precision < 0 || precision > 1) return KG_EINVAL;
+}  // extern "C"
+
+namespace {
+// the all-shell projection into device memory; *out_alm = (L+1) x (2L+1) x Nx complex
+int project_all(kg_solver* h, int L, int precision, double2** out_alm) {
   const int Ny = h->Ny, Nz = h->Nz, Nx = h->Nx;
   const int Nm = (L + 1) * (L + 2) / 2;
   const int K = Ny * Nz;
@@ -1302,7 +1311,80 @@ int kg_project_all_shells(kg_solver* h, int L, int precision, double* host_alm) 
     kg::launch_ylm_fp64(F, Nx, L, Ny, Nz, normP, cosm, sinm, h->sint, dydz, dalm, h->stream);
   }
   KG_CK(cudaGetLastError());
+  *out_alm = dalm;
+  return KG_OK;
+}
+
+int ensure_radial_basis(kg_solver* h, int L, int Nk) {
+  if (h->radL == L && h->radNk == Nk) return KG_OK;
+  const int Nx = h->Nx;
+  kg::bessel_basis(L, Nk, Nx, h->xmin, h->dx, h->r_max, h->rad_k, h->rad_basis);
+  std::vector<double> jr((size_t)(L + 1) * Nx * Nk);
+  for (int l = 0; l <= L; ++l)
+    for (int n = 0; n < Nk; ++n)
+      for (int i = 0; i < Nx; ++i) {
+        const double r = h->xmin + (double)i * h->dx;
+        jr[((size_t)l * Nx + i) * Nk + n] = h->rad_basis[((size_t)l * Nk + n) * Nx + i] * (r * r);
+      }
+  for (void** p : {(void**)&h->rad_jr, (void**)&h->rad_ft})
+    if (*p) {
+      cudaFree(*p);
+      *p = nullptr;
+    }
+  int rc;
+  if ((rc = dalloc(h, (void**)&h->rad_jr, jr.size() * sizeof(double)))) return rc;
+  if ((rc = dalloc(h, (void**)&h->rad_ft, (size_t)Nk * (L + 1) * (2 * L + 1) * sizeof(double2)))) return rc;
+  KG_CK(cudaMemcpyAsync(h->rad_jr, jr.data(), jr.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  h->radL = L;
+  h->radNk = Nk;
+  return KG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int kg_project_all_shells(kg_solver* h, int L, int precision, double* host_alm) {
+  if (!h || !host_alm || L < 0 || L > 128 || precision < 0 || precision > 1) return KG_EINVAL;
+  double2* dalm = nullptr;
+  int rc = project_all(h, L, precision, &dalm);
+  if (rc) return rc;
+  const size_t szAlm = (size_t)(L + 1) * (2 * L + 1) * h->Nx * sizeof(double2);
   KG_CK(cudaMemcpyAsync(host_alm, dalm, szAlm, cudaMemcpyDeviceToHost, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return check_device_flag(h);
+}
+
+int kg_bessel_basis(kg_solver* h, int L, int Nk, double* k_values, double* j_basis) {
+  if (!h || L < 0 || L > 128 || Nk < 1 || Nk > 4096) return KG_EINVAL;
+  int rc = ensure_radial_basis(h, L, Nk);
+  if (rc) return rc;
+  const int NL = L + 1, Nx = h->Nx;
+  for (int l = 0; l <= L; ++l)
+    for (int n = 0; n < Nk; ++n) {
+      if (k_values) k_values[l + (size_t)NL * n] = h->rad_k[(size_t)l * Nk + n];
+      if (j_basis)
+        for (int i = 0; i < Nx; ++i)
+          j_basis[l + (size_t)NL * (n + (size_t)Nk * i)] = h->rad_basis[((size_t)l * Nk + n) * Nx + i];
+    }
+  return KG_OK;
+}
+
+int kg_sph_ft_radial(kg_solver* h, int L, int Nk, int precision, double* host_ft) {
+  if (!h || !host_ft || L < 0 || L > 128 || Nk < 1 || Nk > 4096 || precision < 0 || precision > 1)
+    return KG_EINVAL;
+  int rc = ensure_radial_basis(h, L, Nk);
+  if (rc) return rc;
+  double2* dalm = nullptr;
+  if ((rc = project_all(h, L, precision, &dalm))) return rc;
+  const double dr = std::fabs((h->xmin + h->dx) - h->xmin);
+  {
+    Prof pf(h, PK_RADIAL, 1);
+    kg::launch_radial_ft(dalm, h->rad_jr, L, Nk, h->Nx, dr, h->rad_ft, h->stream);
+  }
+  KG_CK(cudaGetLastError());
+  KG_CK(cudaMemcpyAsync(host_ft, h->rad_ft, (size_t)Nk * (L + 1) * (2 * L + 1) * sizeof(double2),
+                        cudaMemcpyDeviceToHost, h->stream));
   KG_CK(cudaStreamSynchronize(h->stream));
   return check_device_flag(h);
 }

@@ -1,6 +1,7 @@
 // kg_diag.h -- detector-shell tables and launchers of kg_diag.cu
 #pragma once
 #include <cuda_runtime.h>
+#include <vector>
 #include "kg_device.cuh"
 
 namespace kg {
@@ -42,4 +43,12 @@ void launch_ylm_b(int L, int Ny, int Nz, int Kp, const double* normP, const doub
 void launch_ylm_assemble(const float* C, int ldc, int Nx, int L, double dydz, double2* alm, cudaStream_t st);
 void launch_ylm_fp64(const double2* F, int Nx, int L, int Ny, int Nz, const double* normP, const double* cosm,
                      const double* sinm, const double* sint, double dydz, double2* alm, cudaStream_t st);
+
+// spherical-Bessel radial basis and transform (kg_radial.cu)
+double sph_jl(int l, double x);
+void sph_jl_zeros(int L, int Nk, std::vector<double>& z);
+void bessel_basis(int L, int Nk, int Nx, double xmin, double dx, double r_max, std::vector<double>& k_values,
+                  std::vector<double>& basis);
+void launch_radial_ft(const double2* flm, const double* jr, int L, int Nk, int Nx, double dr, double2* ft,
+                      cudaStream_t st);
 }  // namespace kg

@@ -257,6 +257,19 @@ class ScalarField(LinesMethod):
         self._ck(self._lib.kg_project_all_shells(self._h, L, precision, _dp(out.view(np.float64))))
         return out
 
+    def bessel_basis(self, L, Nk):
+        """(k_values (Nk, L+1), j_basis (Nx, Nk, L+1)): generate_full_bessel_basis"""
+        k = np.zeros((Nk, L + 1))
+        jb = np.zeros((self.Nx, Nk, L + 1))
+        self._ck(self._lib.kg_bessel_basis(self._h, L, Nk, _dp(k), _dp(jb)))
+        return k, jb
+
+    def sph_ft_radial(self, L, Nk, precision=0):
+        """SphFT_discrete_radial of phi: array (2L+1, L+1, Nk) complex, [m+L, l, n-1]"""
+        out = np.zeros((2 * L + 1, L + 1, Nk), np.complex128)
+        self._ck(self._lib.kg_sph_ft_radial(self._h, L, Nk, precision, _dp(out.view(np.float64))))
+        return out
+
     def detectors(self):
         r = np.zeros(self.n_det)
         idx = np.zeros(self.n_det, np.int32)

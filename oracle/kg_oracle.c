@@ -910,6 +910,127 @@ void kgo_project_all_shells(const kgo *s, int L, double *alm) {
   free(sl); free(ylm);
 }
 
+/* spherical Bessel j_l(x) (GSL's gsl_sf_bessel_jl in the reference,
+ * tools/FFT_sph.f90:29-34; GSL is not available here): Miller's downward
+ * recurrence j_{k-1} = (2k+1)/x j_k - j_{k+1} from an order above both l and
+ * x, normalised by the closed forms of j_0 or j_1. */
+double kgo_sph_jl(int l, double x) {
+  if (x == 0.0) return l == 0 ? 1.0 : 0.0;
+  double ax = fabs(x), sg = (x < 0.0 && (l & 1)) ? -1.0 : 1.0;
+  double j0 = sin(ax) / ax, j1 = sin(ax) / (ax * ax) - cos(ax) / ax;
+  if (l == 0) return j0;
+  if (l == 1 && ax > 1.0) return sg * j1; /* closed form cancels for small x */
+  double big = (double)l > ax ? (double)l : ax;
+  int top = (int)big + 30 + (int)sqrt(40.0 * big);
+  double jp = 0.0, jc = 1e-30, keep = 0.0;
+  for (int k = top; k >= 1; --k) {
+    double jm = (2.0 * k + 1.0) / ax * jc - jp;
+    jp = jc; jc = jm;
+    if (k - 1 == l) keep = jc;
+    if (fabs(jc) > 1e250) { jc *= 1e-250; jp *= 1e-250; keep *= 1e-250; }
+  }
+  double scale = fabs(j0) >= fabs(j1) ? j0 / jc : j1 / jp;
+  return sg * keep * scale;
+}
+
+/* n-th positive zero of j_l for l = 0..L, n = 1..Nk (gsl_sf_bessel_zero_Jnu(l+1/2, n),
+ * tools/FFT_sph.f90:22-27): zeros of j_0 are n pi, and the zeros of J_nu and
+ * J_{nu+1} interlace, so each zero of j_{l+1} is bisected between two
+ * consecutive zeros of j_l.  z[l*Nk + n-1]. */
+void kgo_sph_jl_zeros(int L, int Nk, double *z) {
+  const double pi = acos(-1.0);
+  int cnt0 = Nk + L;
+  double *prev = xcalloc(cnt0 + 1, sizeof(double)), *cur = xcalloc(cnt0 + 1, sizeof(double));
+  for (int n = 1; n <= cnt0; ++n) prev[n - 1] = n * pi;
+  for (int n = 0; n < Nk; ++n) z[n] = prev[n];
+  for (int l = 1; l <= L; ++l) {
+    int cnt = Nk + L - l;
+    for (int n = 0; n < cnt; ++n) {
+      double lo = prev[n], hi = prev[n + 1], flo = kgo_sph_jl(l, lo);
+      for (int it = 0; it < 200; ++it) {
+        double mid = 0.5 * (lo + hi);
+        if (mid <= lo || mid >= hi) break;
+        double fm = kgo_sph_jl(l, mid);
+        if (fm == 0.0) { lo = hi = mid; break; }
+        if ((fm > 0.0) == (flo > 0.0)) { lo = mid; flo = fm; } else hi = mid;
+      }
+      cur[n] = 0.5 * (lo + hi);
+    }
+    for (int n = 0; n < Nk; ++n) z[(size_t)l * Nk + n] = cur[n];
+    double *t = prev; prev = cur; cur = t;
+  }
+  free(prev); free(cur);
+}
+
+/* generate_full_bessel_basis (tools/FFT_sph.f90:13-95) on the vertex radii
+ * r(i) = xmin + (i-1) dx: k_values(0:L, Nk), j_basis(0:L, Nk, Nx), Fortran
+ * order (l fastest); normalised by sqrt(trapezium_1D(j^2 r^2, dr)). */
+void kgo_bessel_basis(const kgo *s, int L, int Nk, double *k_values, double *j_basis) {
+  const int NL = L + 1, Nx = s->Nx;
+  double *z = xcalloc((size_t)NL * Nk, sizeof(double));
+  kgo_sph_jl_zeros(L, Nk, z);
+  double *r = xcalloc(Nx, sizeof(double)), *jb = xcalloc(Nx, sizeof(double)), *f = xcalloc(Nx, sizeof(double));
+  for (int i = 1; i <= Nx; ++i) r[i - 1] = s->xmin + (double)(i - 1) * s->dx;
+  double dr = fabs(r[1] - r[0]);
+  /* r_max: the outermost point of the evolution grid, x(Nx + g) (MoL/diagnostic_lib.f90:90-92) */
+  const double r_max = s->x1d[s->iR - s->iL];
+  for (int l = 0; l <= L; ++l)
+    for (int n = 1; n <= Nk; ++n) {
+      double kv = z[(size_t)l * Nk + n - 1] / r_max;
+      k_values[l + (size_t)NL * (n - 1)] = kv;
+      for (int i = 0; i < Nx; ++i) jb[i] = kgo_sph_jl(l, kv * r[i]);
+      for (int i = 0; i < Nx; ++i) f[i] = (jb[i] * jb[i]) * (r[i] * r[i]);
+      double sum = 0.0;
+      for (int i = 1; i < Nx - 1; ++i) sum += f[i];
+      double nrm = sqrt(dr * (0.5 * f[0] + sum + 0.5 * f[Nx - 1]));
+      for (int i = 0; i < Nx; ++i)
+        j_basis[l + (size_t)NL * ((n - 1) + (size_t)Nk * i)] = nrm > 0.0 ? jb[i] / nrm : jb[i];
+    }
+  free(z); free(r); free(jb); free(f);
+}
+
+/* SphFT_discrete_radial (tools/FFT_sph.f90:213-244) of phi: ft(1:Nk, 0:L, -L:L),
+ * n fastest; flm from project_sh on every vertex shell, then
+ * trapezium_1D_complex (tools/integral.f90:197-217) of flm j_basis r^2 over r
+ * for n = 1..Nk (the reference's own loop runs n = 0..Nk over a dummy declared
+ * with the wrong shape; this is the contraction of the basis as built). */
+void kgo_sph_ft_radial(const kgo *s, int L, int Nk, double *ft_out) {
+  const int NL = L + 1, NM = 2 * L + 1, Nx = s->Nx;
+  double *k = xcalloc((size_t)NL * Nk, sizeof(double));
+  double *jb = xcalloc((size_t)NL * Nk * Nx, sizeof(double));
+  kgo_bessel_basis(s, L, Nk, k, jb);
+  cplx *flm = xcalloc((size_t)NL * NM * Nx, sizeof(cplx));
+  kgo_project_all_shells(s, L, (double *)flm);
+  cplx *ft = (cplx *)ft_out;
+  double dr = fabs((s->xmin + s->dx) - s->xmin);
+  memset(ft, 0, sizeof(cplx) * (size_t)Nk * NL * NM);
+  for (int l = 0; l <= L; ++l)
+    for (int m = -l; m <= l; ++m)
+      for (int n = 0; n < Nk; ++n) {
+        /* first and last terms with weight 1/2, interior terms in order */
+        cplx sum;
+        {
+          int i0 = 0, i1 = Nx - 1;
+          double r0 = s->xmin, r1 = s->xmin + (double)i1 * s->dx;
+          double w0 = jb[l + (size_t)NL * (n + (size_t)Nk * i0)] * (r0 * r0);
+          double w1 = jb[l + (size_t)NL * (n + (size_t)Nk * i1)] * (r1 * r1);
+          cplx f0 = flm[l + (size_t)NL * ((m + L) + (size_t)NM * i0)];
+          cplx f1 = flm[l + (size_t)NL * ((m + L) + (size_t)NM * i1)];
+          cplx t0 = {w0 * f0.re, w0 * f0.im}, t1 = {w1 * f1.re, w1 * f1.im};
+          sum = rmul(0.5, cadd(t0, t1));
+        }
+        for (int i = 1; i < Nx - 1; ++i) {
+          double r = s->xmin + (double)i * s->dx;
+          double w = jb[l + (size_t)NL * (n + (size_t)Nk * i)] * (r * r);
+          cplx f = flm[l + (size_t)NL * ((m + L) + (size_t)NM * i)];
+          cplx t = {w * f.re, w * f.im};
+          sum = cadd(sum, t);
+        }
+        ft[n + (size_t)Nk * (l + (size_t)NL * (m + L))] = rmul(dr, sum);
+      }
+  free(k); free(jb); free(flm);
+}
+
 /* ------------------------------------------------------------------ */
 /* construction and state access                                       */
 

@@ -66,6 +66,11 @@ def lib():
         L.kgo_currents_detectors.argtypes = [P, D]
         L.kgo_proyector_detectors.argtypes = [P, I, D]
         L.kgo_project_all_shells.argtypes = [P, I, D]
+        L.kgo_sph_jl.argtypes = [I, C.c_double]
+        L.kgo_sph_jl.restype = C.c_double
+        L.kgo_sph_jl_zeros.argtypes = [I, I, D]
+        L.kgo_bessel_basis.argtypes = [P, I, I, D, D]
+        L.kgo_sph_ft_radial.argtypes = [P, I, I, D]
         L.kgo_sph_harmonics.argtypes = [P, I, D]
         L.kgo_project_sh.argtypes = [P, D, D, I, D]
         L.kgo_domain_to_sph_shell.argtypes = [P, D, I, D]
@@ -210,6 +215,19 @@ class Oracle:
         lib().kgo_project_all_shells(self.h, L, _dp(out.view(np.float64)))
         return out
 
+    def bessel_basis(self, L, Nk):
+        """(k_values (Nk, L+1), j_basis (Nx, Nk, L+1))"""
+        k = np.zeros((Nk, L + 1))
+        jb = np.zeros((self.Nx, Nk, L + 1))
+        lib().kgo_bessel_basis(self.h, L, Nk, _dp(k), _dp(jb))
+        return k, jb
+
+    def sph_ft_radial(self, L, Nk):
+        """(2L+1, L+1, Nk) complex, [m+L, l, n-1]"""
+        out = np.zeros((2 * L + 1, L + 1, Nk), np.complex128)
+        lib().kgo_sph_ft_radial(self.h, L, Nk, _dp(out.view(np.float64)))
+        return out
+
     def sph_harmonics(self, L):
         out = np.zeros((self.Nz, self.Ny, 2 * L + 1, L + 1), np.complex128)
         lib().kgo_sph_harmonics(self.h, L, _dp(out.view(np.float64)))
@@ -220,6 +238,17 @@ class Oracle:
         idx = np.zeros(self.n_det, np.int32)
         lib().kgo_get_detectors(self.h, _dp(r), idx.ctypes.data_as(C.POINTER(C.c_int)))
         return r, idx
+
+
+def sph_jl(l, x):
+    return lib().kgo_sph_jl(l, float(x))
+
+
+def sph_jl_zeros(L, Nk):
+    """(L+1, Nk): n-th positive zero of j_l"""
+    z = np.zeros((L + 1, Nk))
+    lib().kgo_sph_jl_zeros(L, Nk, _dp(z))
+    return z
 
 
 def set_threads(n):

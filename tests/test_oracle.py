@@ -247,3 +247,76 @@ def test_all_shell_projection_contains_detector_projection():
     for d, iv in enumerate(idx):
         if iv > 0:
             assert np.array_equal(a_det[d], a_all[iv - 1])
+
+
+def test_spherical_bessel_against_scipy():
+    """j_l (gsl_sf_bessel_jl in the reference, tools/FFT_sph.f90:29-34) against
+    scipy, relative to the function's envelope (|j_l| below l, sqrt(j_l^2 + y_l^2) above)"""
+    from scipy.special import spherical_jn, spherical_yn
+    from oracle.oracle import sph_jl
+    worst = 0.0
+    for l in list(range(0, 12)) + [20, 33, 47, 64, 90, 128]:
+        for x in np.concatenate([np.geomspace(1e-3, 1.0, 9), np.linspace(1.0, 420.0, 160)]):
+            b = spherical_jn(l, x)
+            if abs(b) < 1e-250:
+                continue
+            env = abs(b) if x < l else math.hypot(b, spherical_yn(l, x))
+            worst = max(worst, abs(sph_jl(l, x) - b) / env)
+    assert worst < 1e-12, worst
+
+
+def test_spherical_bessel_zeros_against_scipy():
+    """zeros of j_l (gsl_sf_bessel_zero_Jnu(l + 1/2, n), tools/FFT_sph.f90:22-27)
+    against scipy's brentq on spherical_jn"""
+    from scipy.optimize import brentq
+    from scipy.special import spherical_jn
+    from oracle.oracle import sph_jl_zeros
+    z = sph_jl_zeros(64, 100)
+    for l in (0, 1, 2, 7, 10, 33, 64):
+        for n in (1, 2, 3, 50, 99, 100):
+            zz = z[l, n - 1]
+            r = brentq(lambda x: spherical_jn(l, x), zz - 0.05, zz + 0.05, xtol=1e-15, rtol=1e-15)
+            assert abs(zz - r) <= 4e-15 * r, (l, n, zz, r)
+    # strictly increasing in n, interlaced in l
+    assert np.all(np.diff(z, axis=1) > 0)
+    assert np.all(z[1:, :-1] > z[:-1, :-1]) and np.all(z[1:, :-1] < z[:-1, 1:])
+
+
+def test_bessel_basis_normalised_and_radial_transform_against_numpy():
+    """generate_full_bessel_basis (tools/FFT_sph.f90:13-95): each basis function
+    has unit trapezium norm with weight r^2; SphFT_discrete_radial
+    (tools/FFT_sph.f90:213-244) equals a numpy trapezium of the oracle's
+    all-shell projection against a basis built from scipy's j_l and zeros."""
+    from scipy.optimize import brentq
+    from scipy.special import spherical_jn
+    g = GRID
+    L, Nk = 4, 12
+    o = Oracle(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], m=0.3)
+    o.set_state(_ic())
+    k, jb = o.bessel_basis(L, Nk)
+    sc = o.scalars()
+    r = g["xmin"] + np.arange(g["Nx"]) * sc["dx"]
+    dr = abs(r[1] - r[0])
+    w = np.full(g["Nx"], dr)
+    w[[0, -1]] *= 0.5
+    norms = np.einsum("i,inl,inl->nl", w * r ** 2, jb, jb)
+    assert np.allclose(norms, 1.0, rtol=0, atol=1e-13)
+    # independent basis
+    r_max = g["xmin"] + (g["Nx"] + 4) * sc["dx"]
+    jb_s = np.zeros_like(jb)
+    for l in range(L + 1):
+        zs = []
+        x = 0.5
+        while len(zs) < Nk:
+            if spherical_jn(l, x) * spherical_jn(l, x + 0.05) < 0:
+                zs.append(brentq(lambda t: spherical_jn(l, t), x, x + 0.05, xtol=1e-15, rtol=1e-15))
+            x += 0.05
+        for n, zz in enumerate(zs):
+            assert abs(k[n, l] - zz / r_max) <= 1e-14 * k[n, l]
+            v = spherical_jn(l, zz / r_max * r)
+            jb_s[:, n, l] = v / math.sqrt(np.sum(w * (v * r) ** 2))
+    assert np.abs(jb - jb_s).max() <= 1e-11 * np.abs(jb_s).max()
+    flm = o.project_all_shells(L)                          # (Nx, 2L+1, L+1)
+    ft_np = np.einsum("i,iml,inl->mln", w * r ** 2, flm, jb_s)
+    ft = o.sph_ft_radial(L, Nk)
+    assert np.abs(ft - ft_np).max() <= 1e-11 * np.abs(ft_np).max()
