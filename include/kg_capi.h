@@ -107,6 +107,12 @@ int kg_pirk3(kg_solver *h, int nsteps);
 int kg_rk3(kg_solver *h, int nsteps);
 /* rk4 (:411-474) with the same rhs */
 int kg_rk4(kg_solver *h, int nsteps);
+/* Precision of kg_rk4 on this handle: 0 = FP64 throughout (the reference's
+ * arithmetic, default); 1 = mixed: the stencil RHS in FP32 on FP32 stage states,
+ * u^n and the update u^n + (k1 + 2k2 + 2k3 + k4)/6 in FP64, FP64 RHS on the
+ * excision planes and next to the poles.  The other steppers stay FP64. */
+int kg_set_precision(kg_solver *h, int mode);
+int kg_get_precision(const kg_solver *h);
 /* turn graph replay of multi-step calls on (default) or off */
 int kg_set_graphs(kg_solver *h, int on);
 
@@ -212,6 +218,8 @@ int kg_batch_rk4(kg_batch *b, int nsteps);
 int kg_batch_synchronize(kg_batch *b);
 /* launch shape: phi planes per work item and persistent CTAs (the tuner's knobs) */
 int kg_batch_set_tuning(kg_batch *b, int kchunk, int blocks);
+/* 0 = FP64 RK4 for every member (default), 1 = mixed precision as kg_set_precision */
+int kg_batch_set_precision(kg_batch *b, int mode);
 int kg_batch_get_tuning(const kg_batch *b, int *kchunk, int *blocks);
 long long kg_batch_launch_count(const kg_batch *b);
 void *kg_batch_get_stream(const kg_batch *b);

@@ -23,7 +23,10 @@ from . import capi
 
 
 class Batch:
-    def __init__(self, device=-1):
+    """Solves advanced together by RK4 in one persistent launch per stage.
+    precision: 'fp64' (default) or 'mixed' (FP32 stencil RHS, FP64 state update)."""
+
+    def __init__(self, device=-1, precision="fp64"):
         self._lib = capi.load()
         h = C.c_void_p()
         rc = self._lib.kg_batch_create(device, C.byref(h))
@@ -31,6 +34,11 @@ class Batch:
             raise capi.KgError(rc, "kg_batch_create failed")
         self._b = h
         self.members = []
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision is 'fp64' or 'mixed'")
+        if precision == "mixed":
+            self._ck(self._lib.kg_batch_set_precision(self._b, 1))
+        self.precision = precision
 
     def _ck(self, rc):
         if rc != capi.KG_OK:

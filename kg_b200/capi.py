@@ -59,6 +59,8 @@ SIGNATURES = [
     ("kg_pirk3", _I, [_P, _I]),
     ("kg_rk3", _I, [_P, _I]),
     ("kg_rk4", _I, [_P, _I]),
+    ("kg_set_precision", _I, [_P, _I]),
+    ("kg_get_precision", _I, [_P]),
     ("kg_set_graphs", _I, [_P, _I]),
     ("kg_rhs", _I, [_P, _D, _D, C.c_uint]),
     ("kg_boundary", _I, [_P, C.c_uint]),
@@ -93,6 +95,7 @@ SIGNATURES = [
     ("kg_batch_rk4", _I, [_P, _I]),
     ("kg_batch_synchronize", _I, [_P]),
     ("kg_batch_set_tuning", _I, [_P, _I, _I]),
+    ("kg_batch_set_precision", _I, [_P, _I]),
     ("kg_batch_get_tuning", _I, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("kg_batch_launch_count", C.c_longlong, [_P]),
     ("kg_batch_get_stream", C.c_void_p, [_P]),

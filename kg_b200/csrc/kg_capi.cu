@@ -67,7 +67,11 @@ struct kg_solver {
   // CUDA graphs of two consecutive steps per stepper and Pi-slot state
   int use_graphs = 1;
   struct GraphEntry { cudaGraphExec_t exec = nullptr; int gen = -1; long long launches = 0; };
-  GraphEntry graphs[4][4];               // [stepper][slot state]
+  GraphEntry graphs[5][4];               // [stepper (pirk2, pirk3, rk3, rk4, mixed rk4)][slot state]
+  // mixed precision (RK4): FP32 stage states R1, R2 and increment sum, 5 slots each
+  int precision = 0;                     // 0: FP64, 1: FP32 RHS with FP64 state update
+  float2* MX = nullptr;
+  unsigned char* mx_gdesc = nullptr;     // FP32 ghost-fill descriptors of R1, R2 (device)
   int graph_gen = 0;
   // detectors and projection
   int n_det = 5;
@@ -134,12 +138,13 @@ double2* fld(double2* base, const Grid& g, int v) { return base + (long long)v *
 
 // kernel kinds reported by kg_profile_read: the 13 stage kinds, then these
 enum { PK_GHOST = 13, PK_FACE, PK_RHS, PK_CONVERT, PK_DENSITY, PK_MASS, PK_SHELL, PK_FLUX, PK_PROJECT,
-       PK_YLM_PREP, PK_YLM_GEMM, PK_YLM_FP64, PK_RADIAL, PK_COUNT };
+       PK_YLM_PREP, PK_YLM_GEMM, PK_YLM_FP64, PK_RADIAL, PK_MX1, PK_MX2, PK_MX3, PK_MX4, PK_GHOST_F32, PK_COUNT };
 const char* const kPkNames[PK_COUNT] = {
     "stage_pirk_s1_psi", "stage_pirk_s1_pi", "stage_pirk2_s2", "stage_pirk3_s2_psi", "stage_pirk3_s2_pi",
     "stage_pirk3_s3", "stage_rk3_1", "stage_rk3_2", "stage_rk3_3", "stage_rk4_1", "stage_rk4_2", "stage_rk4_3",
     "stage_rk4_4", "ghost_fill", "boundary_face", "rhs", "layout_convert", "density", "mass_reduce",
-    "shell_interp", "flux_reduce", "ylm_project", "ylm_all_prepare", "ylm_all_gemm_bf16x3", "ylm_all_fp64", "radial_ft"};
+    "shell_interp", "flux_reduce", "ylm_project", "ylm_all_prepare", "ylm_all_gemm_bf16x3", "ylm_all_fp64", "radial_ft", "mixed_rk4_1",
+    "mixed_rk4_2", "mixed_rk4_3", "mixed_rk4_4", "ghost_fill_f32"};
 
 cudaEvent_t take_event(kg_solver* h) {
   if (!h->pool.empty()) {
@@ -736,7 +741,7 @@ int kg_destroy(kg_solver* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   void* bufs[] = {h->dmet, h->U, h->S, h->T, h->RK, h->UP, h->HV, h->stage_buf, h->rho, h->partials,
                   h->d_int, h->d_dbl, h->shells, h->alm, h->flux, h->derr, h->ylm_tab, h->ylm_buf,
-                  h->rad_jr, h->rad_ft};
+                  h->rad_jr, h->rad_ft, h->MX, h->mx_gdesc};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (auto& row : h->graphs)
@@ -951,6 +956,81 @@ int step_rk4(kg_solver* h, int nsteps) {
   return KG_OK;
 }
 
+// FP32 stage buffers and their ghost-fill descriptors
+int ensure_mixed(kg_solver* h) {
+  if (h->MX) return KG_OK;
+  int rc;
+  if ((rc = dalloc(h, (void**)&h->MX, (size_t)15 * h->g.fs * sizeof(float2)))) return rc;
+  const size_t dsz = kg::ghost_f32_desc_bytes();
+  if ((rc = dalloc(h, (void**)&h->mx_gdesc, 2 * dsz))) return rc;
+  std::vector<unsigned char> d(2 * dsz);
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  kg::fill_ghost_f32_desc(d.data(), h->g, h->MX, h->U, inflow);
+  kg::fill_ghost_f32_desc(d.data() + dsz, h->g, h->MX + 5 * h->g.fs, h->U, inflow);
+  KG_CK(cudaMemcpyAsync(h->mx_gdesc, d.data(), d.size(), cudaMemcpyHostToDevice, h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
+kg::MixedLaunch mixed_launch(kg_solver* h) {
+  kg::MixedLaunch L;
+  memset(&L, 0, sizeof(L));
+  L.g = h->g;
+  L.m = metric_of(h);
+  L.metric_kind = h->p.metric == KG_SCHW_EF ? kg::MK_SCHW : kg::MK_KS;
+  L.base = h->U;
+  L.acc = h->MX + 10 * h->g.fs;
+  return L;
+}
+
+int run_mixed_stage(kg_solver* h, int st, const kg::MixedLaunch& L) {
+  static const int kinds[4] = {kg::ST_RK4_1, kg::ST_RK4_2, kg::ST_RK4_3, kg::ST_RK4_4};
+  Prof pf(h, PK_MX1 + st, 1);
+  const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
+  if (kg::launch_stage_mixed(kinds[st], L, rsg, h->derr, h->stream))
+    return set_err(h, KG_ECUDA, "mixed-precision stage could not be configured (tensor maps)");
+  return KG_OK;
+}
+
+void run_ghost_f32(kg_solver* h, int which) {
+  Prof pf(h, PK_GHOST_F32, 2);
+  const Grid& g = h->g;
+  kg::launch_ghost_fill_f32(h->mx_gdesc + which * kg::ghost_f32_desc_bytes(), 1, 6LL * g.NK * g.NI,
+                            2LL * (g.NJ - 6) * g.NK, 2LL * g.NI * g.NJ, h->stream);
+}
+
+// RK4 with the stencil RHS in FP32 and the state update in FP64 (kg_mixed.cu)
+int step_rk4_mixed(kg_solver* h, int nsteps) {
+  int rc;
+  if ((rc = ensure_mixed(h))) return rc;
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  float2* R1 = h->MX;
+  float2* R2 = h->MX + 5 * h->g.fs;
+  for (int s = 0; s < nsteps; ++s) {
+    kg::MixedLaunch L = mixed_launch(h);
+    L.out_f = R1;
+    if ((rc = run_mixed_stage(h, 0, L))) return rc;
+    run_ghost_f32(h, 0);
+    L.in_f = R1;
+    L.out_f = R2;
+    if ((rc = run_mixed_stage(h, 1, L))) return rc;
+    run_ghost_f32(h, 1);
+    L.in_f = R2;
+    L.out_f = R1;
+    if ((rc = run_mixed_stage(h, 2, L))) return rc;
+    run_ghost_f32(h, 0);
+    L.in_f = R1;
+    L.out_f = nullptr;
+    L.out_d = h->U;
+    L.skip_last_i = inflow;
+    if ((rc = run_mixed_stage(h, 3, L))) return rc;
+    run_ghost(h, h->U, h->U, inflow);
+    h->t = h->t + h->dt;
+  }
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
 // Runs nsteps steps.  Pairs of steps are replayed from a CUDA graph captured
 // once per stepper and Pi-slot state (two steps return the PIRK slots to the
 // state they started in); an odd last step, or runs with profiling on, launch
@@ -1015,7 +1095,19 @@ int run_steps(kg_solver* h, int which, int nsteps, int (*step)(kg_solver*, int))
 int kg_pirk2(kg_solver* h, int nsteps) { return run_steps(h, 0, nsteps, step_pirk2); }
 int kg_pirk3(kg_solver* h, int nsteps) { return run_steps(h, 1, nsteps, step_pirk3); }
 int kg_rk3(kg_solver* h, int nsteps) { return run_steps(h, 2, nsteps, step_rk3); }
-int kg_rk4(kg_solver* h, int nsteps) { return run_steps(h, 3, nsteps, step_rk4); }
+int kg_rk4(kg_solver* h, int nsteps) {
+  if (h && h->precision == 1) return run_steps(h, 4, nsteps, step_rk4_mixed);
+  return run_steps(h, 3, nsteps, step_rk4);
+}
+
+int kg_set_precision(kg_solver* h, int mode) {
+  if (!h || mode < 0 || mode > 1) return KG_EINVAL;
+  if (mode == 1 && !kg::tma_available(h->g, h->U)) return set_err(h, KG_EINVAL, "tensor maps unavailable");
+  h->precision = mode;
+  return KG_OK;
+}
+
+int kg_get_precision(const kg_solver* h) { return h ? h->precision : -1; }
 
 int kg_set_graphs(kg_solver* h, int on) {
   if (!h) return KG_EINVAL;
@@ -1477,6 +1569,8 @@ struct kg_batch {
   // per RK4 stage: item records and ghost descriptors (device)
   unsigned char* ditems[4] = {nullptr, nullptr, nullptr, nullptr};
   kg::GhostDesc* dghost[4] = {nullptr, nullptr, nullptr, nullptr};
+  unsigned char* dghost_f[3] = {nullptr, nullptr, nullptr};  // FP32 stage fills (mixed precision)
+  int precision = 0;                                         // 0: FP64 RK4, 1: mixed (kg_mixed.cu)
   size_t items_cap = 0, ghost_cap = 0;
   int n_items[4] = {0, 0, 0, 0};
   long long max_rows = 0, max_faces = 0, max_z = 0;
@@ -1500,7 +1594,10 @@ namespace {
 
 int batch_rebuild(kg_batch* b) {
   const int n = (int)b->members.size();
-  const size_t isz = kg::batch_item_bytes();
+  const bool mixed = b->precision == 1;
+  const size_t isz = mixed ? kg::mixed_item_bytes() : kg::batch_item_bytes();
+  const size_t isz_max = std::max(kg::mixed_item_bytes(), kg::batch_item_bytes());
+  const size_t gfsz = kg::ghost_f32_desc_bytes();
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
@@ -1512,15 +1609,21 @@ int batch_rebuild(kg_batch* b) {
       b->ditems[st] = nullptr;
       b->dghost[st] = nullptr;
     }
+    for (int st = 0; st < 3; ++st) {
+      if (b->dghost_f[st]) cudaFree(b->dghost_f[st]);
+      b->dghost_f[st] = nullptr;
+    }
     size_t cap = n < 16 ? 16 : (size_t)n * 2;
     for (int st = 0; st < 4; ++st) {
-      KG_BCK(cudaMalloc((void**)&b->ditems[st], cap * isz));
+      KG_BCK(cudaMalloc((void**)&b->ditems[st], cap * isz_max));
       KG_BCK(cudaMalloc((void**)&b->dghost[st], cap * sizeof(kg::GhostDesc)));
     }
+    for (int st = 0; st < 3; ++st) KG_BCK(cudaMalloc((void**)&b->dghost_f[st], cap * gfsz));
     b->items_cap = cap;
   }
   std::vector<unsigned char> hitems((size_t)n * isz);
   std::vector<kg::GhostDesc> hg(n);
+  std::vector<unsigned char> hgf((size_t)n * gfsz);
   const int kinds[4] = {kg::ST_RK4_1, kg::ST_RK4_2, kg::ST_RK4_3, kg::ST_RK4_4};
   b->max_rows = b->max_faces = b->max_z = 0;
   for (int st = 0; st < 4; ++st) {
@@ -1528,6 +1631,35 @@ int batch_rebuild(kg_batch* b) {
     for (int i = 0; i < n; ++i) {
       kg_solver* h = b->members[i];
       const Grid& g = h->g;
+      if (mixed) {
+        const int inflow = h->p.bc_rmax == KG_INFLOW;
+        float2* F1 = h->MX;
+        float2* F2 = h->MX + 5 * g.fs;
+        kg::MixedLaunch M = mixed_launch(h);
+        M.in_f = st == 1 ? F1 : (st == 2 ? F2 : (st == 3 ? F1 : nullptr));
+        M.out_f = st == 0 ? F1 : (st == 1 ? F2 : (st == 2 ? F1 : nullptr));
+        M.out_d = st == 3 ? h->U : nullptr;
+        M.skip_last_i = st == 3 ? inflow : 0;
+        const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
+        const int ni = kg::build_mixed_item(hitems.data() + (size_t)i * isz, kinds[st], M, rsg, b->derr, b->kchunk,
+                                            item0);
+        if (ni < 0) {
+          b->err = "tensor-map encoding failed for a batch member";
+          return KG_ECUDA;
+        }
+        item0 += ni;
+        if (st < 3) kg::fill_ghost_f32_desc(hgf.data() + (size_t)i * gfsz, g, M.out_f, h->U, inflow);
+        hg[i].g = g;
+        hg[i].u = h->U;
+        hg[i].up = h->U;
+        hg[i].inflow = inflow;
+        if (st == 0) {
+          b->max_rows = std::max(b->max_rows, 6LL * g.NK * g.NI);
+          b->max_faces = std::max(b->max_faces, 2LL * (g.NJ - 6) * g.NK);
+          b->max_z = std::max(b->max_z, 2LL * g.NI * g.NJ);
+        }
+        continue;
+      }
       double2* R1 = h->RK;
       double2* R2 = fld(h->RK, g, 5);
       double2* A = fld(h->RK, g, 10);
@@ -1561,6 +1693,8 @@ int batch_rebuild(kg_batch* b) {
     KG_BCK(cudaMemcpyAsync(b->ditems[st], hitems.data(), (size_t)n * isz, cudaMemcpyHostToDevice, b->stream));
     KG_BCK(cudaMemcpyAsync(b->dghost[st], hg.data(), (size_t)n * sizeof(kg::GhostDesc), cudaMemcpyHostToDevice,
                            b->stream));
+    if (mixed && st < 3)
+      KG_BCK(cudaMemcpyAsync(b->dghost_f[st], hgf.data(), (size_t)n * gfsz, cudaMemcpyHostToDevice, b->stream));
   }
   KG_BCK(cudaStreamSynchronize(b->stream));
   b->dirty = false;
@@ -1571,11 +1705,19 @@ int batch_enqueue_step(kg_batch* b) {
   const int n = (int)b->members.size();
   const int kinds[4] = {kg::ST_RK4_1, kg::ST_RK4_2, kg::ST_RK4_3, kg::ST_RK4_4};
   for (int st = 0; st < 4; ++st) {
-    if (kg::launch_batch_tma(kinds[st], b->metric_kind, b->ditems[st], n, b->n_items[st], b->blocks, b->stream)) {
+    const int bad = b->precision == 1
+                        ? kg::launch_batch_mixed(kinds[st], b->metric_kind, b->ditems[st], n, b->n_items[st],
+                                                 b->blocks, b->stream)
+                        : kg::launch_batch_tma(kinds[st], b->metric_kind, b->ditems[st], n, b->n_items[st],
+                                               b->blocks, b->stream);
+    if (bad) {
       b->err = "batched stage launch could not be configured";
       return KG_ECUDA;
     }
-    kg::launch_ghost_fill_batch(b->dghost[st], n, b->max_rows, b->max_faces, b->max_z, b->stream);
+    if (b->precision == 1 && st < 3)
+      kg::launch_ghost_fill_f32(b->dghost_f[st], n, b->max_rows, b->max_faces, b->max_z, b->stream);
+    else
+      kg::launch_ghost_fill_batch(b->dghost[st], n, b->max_rows, b->max_faces, b->max_z, b->stream);
     b->launches += 3;
   }
   KG_BCK(cudaGetLastError());
@@ -1619,6 +1761,8 @@ int kg_batch_destroy(kg_batch* b) {
     if (b->ditems[st]) cudaFree(b->ditems[st]);
     if (b->dghost[st]) cudaFree(b->dghost[st]);
   }
+  for (int st = 0; st < 3; ++st)
+    if (b->dghost_f[st]) cudaFree(b->dghost_f[st]);
   if (b->derr) cudaFree(b->derr);
   if (b->ev) cudaEventDestroy(b->ev);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -1639,7 +1783,7 @@ int kg_batch_add(kg_batch* b, kg_solver* h) {
   for (kg_solver* m : b->members)
     if (m == h) return KG_OK;
   int rc;
-  if ((rc = ensure(h, &h->RK, 15))) return rc;
+  if ((rc = b->precision == 1 ? ensure_mixed(h) : ensure(h, &h->RK, 15))) return rc;
   if (!kg::tma_available(h->g, h->U)) {
     b->err = "tensor maps unavailable for this grid";
     return KG_EINVAL;
@@ -1735,6 +1879,22 @@ int kg_batch_set_tuning(kg_batch* b, int kchunk, int blocks) {
     b->blocks = blocks;
     b->dirty = true;
   }
+  return KG_OK;
+}
+
+int kg_batch_set_precision(kg_batch* b, int mode) {
+  if (!b || mode < 0 || mode > 1) return KG_EINVAL;
+  if (mode == b->precision) return KG_OK;
+  KG_BCK(cudaStreamSynchronize(b->stream));
+  for (kg_solver* h : b->members) {
+    const int rc = mode == 1 ? ensure_mixed(h) : ensure(h, &h->RK, 15);
+    if (rc) {
+      b->err = "could not allocate stage buffers of a member: " + h->err;
+      return rc;
+    }
+  }
+  b->precision = mode;
+  b->dirty = true;
   return KG_OK;
 }
 

@@ -61,6 +61,27 @@ struct GhostDesc {
 };
 void launch_ghost_fill_batch(const GhostDesc* d_desc, int n, long long max_rows, long long max_faces,
                              long long max_zplanes, cudaStream_t st);
+// mixed-precision RK4 (kg_mixed.cu): FP32 stage states and increment sum, FP64 u
+struct MixedLaunch {
+  Grid g;
+  Metric m;
+  int metric_kind;
+  const float2* in_f;    // stage input of stages 2-4 (5 variables, stride g.fs)
+  const double2* base;   // u^n; the stencil input of stage 1
+  float2* acc;           // k1 + 2 k2 + 2 k3
+  float2* out_f;         // stage output of stages 1-3
+  double2* out_d;        // u^{n+1} (stage 4)
+  int skip_last_i;
+};
+int launch_stage_mixed(int kind, const MixedLaunch& L, const double* rsg, int* err, cudaStream_t st);
+size_t mixed_item_bytes();
+int build_mixed_item(void* dst, int kind, const MixedLaunch& L, const double* rsg, int* err, int kchunk, int item0);
+int launch_batch_mixed(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks,
+                       cudaStream_t st);
+size_t ghost_f32_desc_bytes();
+void fill_ghost_f32_desc(void* dst, const Grid& g, float2* u, const double2* up, int inflow);
+void launch_ghost_fill_f32(const void* d_desc, int n, long long max_rows, long long max_faces, long long max_z,
+                           cudaStream_t st);
 void launch_rhs(const Grid& g, const Metric& m, int metric_kind, const double2* const in[5], double2* out,
                 unsigned mask, cudaStream_t st);
 

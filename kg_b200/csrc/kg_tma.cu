@@ -28,8 +28,10 @@
 #include <cstring>
 #include "kg_device.cuh"
 #include "kg_internal.h"
+#include "kg_tma_ops.cuh"
 
 namespace kg {
+using namespace tmaops;
 namespace {
 
 constexpr int TI = 32, TJ = 8, RH = 2;
@@ -43,49 +45,6 @@ constexpr int MW = TI + 2 * RH, MH = TJ + 2;  // metric tile
 constexpr int MT_N = MW * MH;
 enum { MT_AL = 0, MT_BE, MT_A, MT_GRR, MT_GRP, MT_SG, MT_HT, MT_COUNT };
 constexpr size_t SMEM_BYTES = (size_t)NST * STAGE_B + (size_t)MT_COUNT * MT_N * 8 + 64 + 128;
-constexpr long long WAIT_LIMIT = 1LL << 24;
-
-__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(saddr(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity) {
-  for (long long it = 0; it < WAIT_LIMIT; ++it)
-    if (mbar_try_wait(b, parity)) return true;
-  return false;
-}
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
-                                            uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(saddr(dst)),
-      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(saddr(bar))
-      : "memory");
-}
-
-// L2 prefetch of a tensor box (no shared memory, no completion to wait for)
-__device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap* tm, int c0, int c1, int c2, int c3) {
-  asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(
-                   reinterpret_cast<uint64_t>(tm)),
-               "r"(c0), "r"(c1), "r"(c2), "r"(c3)
-               : "memory");
-}
-
 __device__ __forceinline__ double ddiv(double a, double b, double rb) {
   const double q = a * rb;
   const double r = __fma_rn(-q, b, a);

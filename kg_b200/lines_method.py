@@ -134,6 +134,17 @@ class LinesMethod:
             raise NotImplementedError("a host rhs callback cannot run inside the device stepper")
         self._ck(self._lib.kg_rk4(self._h, nsteps))
 
+    @property
+    def precision(self):
+        """'fp64' (default) or 'mixed' (rk4: FP32 stencil RHS, FP64 state update)"""
+        return "mixed" if self._lib.kg_get_precision(self._h) == 1 else "fp64"
+
+    @precision.setter
+    def precision(self, mode):
+        if mode not in ("fp64", "mixed"):
+            raise ValueError("precision is 'fp64' or 'mixed'")
+        self._ck(self._lib.kg_set_precision(self._h, 1 if mode == "mixed" else 0))
+
     def synchronize(self):
         """Wait for the handle's queued device work (steppers return asynchronously)."""
         self._ck(self._lib.kg_synchronize(self._h))
