@@ -155,7 +155,8 @@ def cpu_baseline(w, threads, nx_sample=128, steps=150):
     return gpsu, dt, f"PIRK2 x{steps} on the Nx={Nx} radial slab of the workload grid ({Nx}x{w['Ny']}x{w['Nz']})"
 
 
-SERVE_DESC = ("scaled serving workload: Poisson arrivals at 60/s, Nr ~ U{128..512 step 64} on r in "
+SERVE_DESC = ("scaled serving workload: Poisson arrivals at 2000/s (the offered load exceeds one GPU's "
+              "capacity, so solves/s measures sustained throughput), Nr ~ U{128..512 step 64} on r in "
               "[1.8, 1.8+0.1 Nr], Ntheta in {16, 32}, Nphi = 2 Ntheta, m ~ U[0, 0.5], shell r0 ~ U[6, 15], "
               "sigma ~ U[0.8, 2], c_lm (l<=4) N(0, 1e-4), RK4, steps log-uniform [100, 1000] (multiples of 10), "
               "l<=8 waveform at r_ext = 0.8 r_max every 10 steps, 160 GB HBM admission budget; the full serving "
@@ -164,20 +165,95 @@ SERVE_DESC = ("scaled serving workload: Poisson arrivals at 60/s, Nr ~ U{128..51
 
 
 def serve_leg(count, device):
-    """plain FP64 (one solve at a time) vs continuous batching on the same requests"""
-    from kg_b200.serve import Server, draw_requests, waveform_error
+    """plain FP64 (one solve at a time) vs continuous batching, FP64 and mixed, on the same requests"""
+    from kg_b200.serve import Server, draw_requests, waveform_error_detail
     from kg_b200.batch import autotune
-    reqs = draw_requests(seed=20240602, rate=60.0, count=count, nr=(128, 512), nr_step=64, ntheta=(16, 32),
+    reqs = draw_requests(seed=20240602, rate=2000.0, count=count, nr=(128, 512), nr_step=64, ntheta=(16, 32),
                          steps=(100, 1000), quantum=10)
     shapes = sorted({(r.grid()["Nx"], r.grid()["Ny"], r.grid()["Nz"]) for r in reqs})
     tune = autotune(shapes[:: max(1, len(shapes) // 6)], device=device, kchunks=(16, 32, 64), steps=2)
-    batched = Server(mode="batched", device=device, tuning=tune).run(reqs)
     plain = Server(mode="plain", device=device).run(reqs)
+    batched = Server(mode="batched", device=device, tuning=tune).run(reqs)
+    mixed = Server(mode="batched", device=device, tuning=tune, precision="mixed").run(reqs)
     strip = lambda d: {k: d[k] for k in ("completed", "wall_s", "solves_per_s", "p50_s", "p99_s") if k in d}
-    out = {"workload": SERVE_DESC, "requests": count, "plain_fp64": strip(plain),
-           "batched_fp64": dict(strip(batched), peak_live=batched.get("peak_live"), tuning=list(tune)),
-           "speedup_solves_per_s": batched["solves_per_s"] / plain["solves_per_s"],
-           "waveform_rel_l2_batched_vs_plain": waveform_error(batched, plain)}
+    return {"workload": SERVE_DESC, "requests": count, "plain_fp64": strip(plain),
+            "batched_fp64": dict(strip(batched), peak_live=batched.get("peak_live"), tuning=list(tune)),
+            "batched_mixed": dict(strip(mixed), peak_live=mixed.get("peak_live")),
+            "speedup_batched_fp64": batched["solves_per_s"] / plain["solves_per_s"],
+            "speedup_batched_mixed": mixed["solves_per_s"] / plain["solves_per_s"],
+            "waveform_batched_fp64_vs_plain": _wave(waveform_error_detail(batched, plain)),
+            "waveform_batched_mixed_vs_plain_fp64": _wave(waveform_error_detail(mixed, plain))}
+
+
+def _wave(d):
+    return {"max_rel_l2": d[0], "requests_compared": d[1], "max_abs_l2": d[2],
+            "note": "relative error over requests whose FP64 waveform norm exceeds 1e-10; absolute over all"}
+
+
+def precision_leg(w, device, steps=40, every=10, L=64):
+    """The precision form on the workload grid: RK4 with the FP32 stencil RHS and
+    FP64 state update, a split-BF16 tensor-core Y_lm projection (l <= L, every
+    shell) every `every` steps, against the FP64 RK4 run with the FP64
+    projection, from the same initial data.  Throughput is device time of the
+    steps plus projections; errors are those of the final projection, of the
+    l <= 8 detector waveform at r = 50 over the run, and of phi and Pi."""
+    import torch
+    from kg_b200 import ScalarField
+    from kg_b200.initial_data import shell_ylm_device
+    out = {}
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        s = ScalarField(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], m=w["m"], device=device,
+                        l_max=8, n_det=1)
+        u0, _ = shell_ylm_device(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], seed=w["seed"],
+                                 device=f"cuda:{device}")
+        s._ck(s._lib.kg_set_state_device(s.handle, 0, C.c_void_p(u0.data_ptr())))
+        s.synchronize()
+        del u0
+        s.set_detectors([50.0])
+        s.precision = prec
+        lib, h = s._lib, s.handle
+        stream = torch.cuda.ExternalStream(lib.kg_get_stream(h), device=f"cuda:{device}")
+        alm_p = 1 if prec == "mixed" else 0
+        host = np.zeros((w["Nx"], 2 * L + 1, L + 1), np.complex128)
+        s.rk4(nsteps=2)  # warm: buffers, graphs
+        s._ck(lib.kg_project_all_shells(h, L, alm_p, host.ctypes.data_as(C.POINTER(C.c_double))))
+        s.synchronize()
+        wave = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dev_ms = 0.0
+        for q in range(steps // every):
+            e0.record(stream)
+            s.rk4(nsteps=every)
+            # projection kernels only (the host copy of the coefficients is outside the timed region)
+            s._ck(lib.kg_project_all_shells(h, L, alm_p, host.ctypes.data_as(C.POINTER(C.c_double))))
+            e1.record(stream)
+            e1.synchronize()
+            dev_ms += e0.elapsed_time(e1)
+            wave.append(s.proyector_detectors()[0].copy())
+        st = torch.empty((w["Nz"] + 1, w["Ny"] + 5, w["Nx"] + 5, 5), dtype=torch.complex128,
+                         device=f"cuda:{device}")
+        s._ck(lib.kg_get_state_device(h, 0, C.c_void_p(st.data_ptr())))
+        s.synchronize()
+        runs[prec] = dict(ms=dev_ms, alm=host.copy(), wave=np.array(wave), phi=st[..., 0].clone(),
+                          pi=st[..., 4].clone())
+        del st
+        s.close()
+        torch.cuda.empty_cache()
+    pts = interior_points(w) * 4 * steps
+    a, b = runs["fp64"], runs["mixed"]
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    trel = lambda x, y: float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y))
+    wave_mode = np.linalg.norm(b["wave"] - a["wave"], axis=0) / np.maximum(np.linalg.norm(a["wave"], axis=0), 1e-300)
+    big = np.linalg.norm(a["wave"], axis=0) > 1e-3 * np.linalg.norm(a["wave"], axis=0).max()
+    out = {"workload": f"RK4 on the {w['Nx']}x{w['Ny']}x{w['Nz']} grid, {steps} steps, all-shell Y_lm projection "
+                       f"(l<={L}) every {every} steps; detector at r=50",
+           "fp64_gpsu": pts / (a["ms"] / 1e3), "mixed_gpsu": pts / (b["ms"] / 1e3),
+           "speedup": a["ms"] / b["ms"],
+           "phi_rel_l2_err": trel(b["phi"], a["phi"]), "pi_rel_l2_err": trel(b["pi"], a["pi"]),
+           "waveform_rel_l2_err_l8_r50": rel(b["wave"], a["wave"]),
+           "waveform_max_per_mode_rel_err": float(wave_mode[big].max()) if big.any() else None,
+           "projection_energy_norm_rel_err": rel(b["alm"], a["alm"])}
     return out
 
 
@@ -293,6 +369,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--serve-count", type=int, default=120)
     ap.add_argument("--no-projection", action="store_true", help="skip the all-shell Y_lm projection leg")
+    ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision leg")
     args = ap.parse_args()
     if args.grid:
         nx, ny, nz = (int(v) for v in args.grid.split(","))
@@ -434,9 +511,13 @@ def main():
             "gpu_launches": int(launches), "clocks": clk}
     if rank == 0 and world == 1 and not args.no_projection:
         line["projection"] = projection_leg(mol, lib, h)
-    if rank == 0 and world == 1 and not args.no_serve and not args.grid:
-        mol.close()
-        line["serving"] = serve_leg(args.serve_count, local)
+    if rank == 0 and world == 1 and not args.grid and not (args.no_precision and args.no_serve):
+        mol.close()  # the legs below allocate their own solves
+        torch.cuda.empty_cache()
+        if not args.no_precision:
+            line["precision"] = precision_leg(w, local)
+        if not args.no_serve:
+            line["serving"] = serve_leg(args.serve_count, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, secs, sample = cpu_baseline(w, threads)
