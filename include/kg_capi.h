@@ -113,6 +113,18 @@ int kg_rk4(kg_solver *h, int nsteps);
  * excision planes and next to the poles.  The other steppers stay FP64. */
 int kg_set_precision(kg_solver *h, int mode);
 int kg_get_precision(const kg_solver *h);
+/* Method of kg_rk4: 0 = the reference's second-order scheme (default);
+ * 1 = configured: fourth-order centred differences (the stencil of
+ * first_derivative_x_4, tools/finite_differences.f90:124-154, with its one-sided
+ * r closures), sixth-order Kreiss-Oliger dissipation of strength ko_eps, a
+ * Sommerfeld condition on the outermost r plane and parity-correct pole ghosts
+ * (psi_2 negated).  Kerr_Schild form, FP64, kg_rk4 only (other steppers return
+ * KG_EINVAL while it is set). */
+int kg_set_scheme(kg_solver *h, int scheme, double ko_eps);
+int kg_get_scheme(const kg_solver *h);
+/* the configured method's ghost fills applied to u (after a kg_set_state of
+ * initial data that does not already satisfy them) */
+int kg_fill_ghosts_cfg(kg_solver *h);
 /* turn graph replay of multi-step calls on (default) or off */
 int kg_set_graphs(kg_solver *h, int on);
 

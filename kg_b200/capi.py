@@ -61,6 +61,9 @@ SIGNATURES = [
     ("kg_rk4", _I, [_P, _I]),
     ("kg_set_precision", _I, [_P, _I]),
     ("kg_get_precision", _I, [_P]),
+    ("kg_set_scheme", _I, [_P, _I, C.c_double]),
+    ("kg_get_scheme", _I, [_P]),
+    ("kg_fill_ghosts_cfg", _I, [_P]),
     ("kg_set_graphs", _I, [_P, _I]),
     ("kg_rhs", _I, [_P, _D, _D, C.c_uint]),
     ("kg_boundary", _I, [_P, C.c_uint]),

@@ -30,7 +30,7 @@ const char* kg_noalloc_last_error();  // kg_noalloc.cu
 namespace {
 
 enum { T_ALPHA = 0, T_BETA, T_DXBETA, T_SQRTG, T_ASG, T_GRR, T_GRP, T_GPP, T_ASG_GTT, T_ASG_GRR, T_A_GPP, T_AM2,
-       T_GTT, T_RSG, T_COUNT };
+       T_GTT, T_RSG, T_DXBETA4, T_COUNT };
 
 }  // namespace
 
@@ -67,7 +67,10 @@ struct kg_solver {
   // CUDA graphs of two consecutive steps per stepper and Pi-slot state
   int use_graphs = 1;
   struct GraphEntry { cudaGraphExec_t exec = nullptr; int gen = -1; long long launches = 0; };
-  GraphEntry graphs[5][4];               // [stepper (pirk2, pirk3, rk3, rk4, mixed rk4)][slot state]
+  GraphEntry graphs[6][4];               // [stepper (pirk2, pirk3, rk3, rk4, mixed rk4, configured rk4)][slot]
+  // method: 0 = the reference's second-order scheme, 1 = configured fourth-order (kg_config.cu)
+  int scheme = 0;
+  double ko_eps = 0.02;
   // mixed precision (RK4): FP32 stage states R1, R2 and increment sum, 5 slots each
   int precision = 0;                     // 0: FP64, 1: FP32 RHS with FP64 state update
   float2* MX = nullptr;
@@ -337,6 +340,18 @@ void derive_tables(kg_solver* h) {
     TB(T_A_GPP, q) = TB(T_ALPHA, q) * TB(T_GPP, q);
     TB(T_AM2, q) = TB(T_ALPHA, q) * m2;
     TB(T_RSG, q) = 1.0 / TB(T_SQRTG, q);  // correctly rounded reciprocal for the Markstein quotient
+  }
+  // d_r beta^r by first_derivative_x_4 (tools/finite_differences.f90:124-154), for the configured method
+  const int NI = h->NI, NJ = h->NJ, n = NI - 1;
+  const double res = 1.0 / (12.0 * h->dx);
+  for (int jj = 0; jj < NJ; ++jj) {
+    const double* F = h->tables.data() + (size_t)T_BETA * n2 + (size_t)NI * jj;
+    double* D = h->tables.data() + (size_t)T_DXBETA4 * n2 + (size_t)NI * jj;
+    D[0] = (-25.0 * F[0] + 48.0 * F[1] - 36.0 * F[2] + 16.0 * F[3] - 3.0 * F[4]) * res;
+    D[1] = (-3.0 * F[0] - 10.0 * F[1] + 18.0 * F[2] - 6.0 * F[3] + 1.0 * F[4]) * res;
+    for (int o = 2; o <= n - 2; ++o) D[o] = (F[o - 2] - 8.0 * F[o - 1] + 8.0 * F[o + 1] - F[o + 2]) * res;
+    D[n - 1] = (3.0 * F[n] + 10.0 * F[n - 1] - 18.0 * F[n - 2] + 6.0 * F[n - 3] - 1.0 * F[n - 4]) * res;
+    D[n] = (25.0 * F[n] - 48.0 * F[n - 1] + 36.0 * F[n - 2] - 16.0 * F[n - 3] + 3.0 * F[n - 4]) * res;
   }
 }
 
@@ -1031,6 +1046,43 @@ int step_rk4_mixed(kg_solver* h, int nsteps) {
   return KG_OK;
 }
 
+// RK4 of the configured method (fourth-order differences, Kreiss-Oliger
+// dissipation, Sommerfeld outer plane; kg_config.cu)
+int step_rk4_cfg(kg_solver* h, int nsteps) {
+  int rc;
+  if ((rc = ensure(h, &h->RK, 15))) return rc;
+  const Grid& g = h->g;
+  double2* R1 = h->RK;
+  double2* R2 = fld(h->RK, g, 5);
+  double2* A = fld(h->RK, g, 10);
+  const double* dxb4 = h->dmet + (size_t)T_DXBETA4 * h->NJ * h->PI;
+  const double coef[6] = {1.0 / (12.0 * h->dx), 1.0 / (12.0 * h->dy), 1.0 / (12.0 * h->dz),
+                          h->ko_eps / (64.0 * h->dx), h->ko_eps / (64.0 * h->dy), h->ko_eps / (64.0 * h->dz)};
+  const double rN = h->x1d[h->NI - 1];
+  static const int kinds[4] = {kg::ST_RK4_1, kg::ST_RK4_2, kg::ST_RK4_3, kg::ST_RK4_4};
+  for (int s = 0; s < nsteps; ++s) {
+    kg::StageLaunch L = base_launch(h);
+    L.base = h->U;
+    L.acc = A;
+    double2* ins[4] = {h->U, R1, R2, R1};
+    double2* outs[4] = {R1, R2, R1, h->U};
+    for (int st = 0; st < 4; ++st) {
+      set_in(L, g, ins[st], fld(ins[st], g, 4));
+      L.out = outs[st];
+      {
+        Prof pf(h, kg::ST_RK4_1 + st, 1);
+        if (kg::launch_stage_cfg(kinds[st], L, dxb4, coef, rN, h->stream))
+          return set_err(h, KG_ECUDA, "configured stage could not be launched");
+      }
+      Prof pg(h, PK_GHOST, 2);
+      kg::launch_ghost_fill_cfg(g, outs[st], h->stream);
+    }
+    h->t = h->t + h->dt;
+  }
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
 // Runs nsteps steps.  Pairs of steps are replayed from a CUDA graph captured
 // once per stepper and Pi-slot state (two steps return the PIRK slots to the
 // state they started in); an odd last step, or runs with profiling on, launch
@@ -1092,16 +1144,43 @@ int run_steps(kg_solver* h, int which, int nsteps, int (*step)(kg_solver*, int))
 
 }  // namespace
 
-int kg_pirk2(kg_solver* h, int nsteps) { return run_steps(h, 0, nsteps, step_pirk2); }
-int kg_pirk3(kg_solver* h, int nsteps) { return run_steps(h, 1, nsteps, step_pirk3); }
-int kg_rk3(kg_solver* h, int nsteps) { return run_steps(h, 2, nsteps, step_rk3); }
+static int only_rk4(kg_solver* h) {
+  return set_err(h, KG_EINVAL, "the configured method (kg_set_scheme 1) runs with kg_rk4 only");
+}
+int kg_pirk2(kg_solver* h, int nsteps) { return h && h->scheme ? only_rk4(h) : run_steps(h, 0, nsteps, step_pirk2); }
+int kg_pirk3(kg_solver* h, int nsteps) { return h && h->scheme ? only_rk4(h) : run_steps(h, 1, nsteps, step_pirk3); }
+int kg_rk3(kg_solver* h, int nsteps) { return h && h->scheme ? only_rk4(h) : run_steps(h, 2, nsteps, step_rk3); }
 int kg_rk4(kg_solver* h, int nsteps) {
+  if (h && h->scheme == 1) return run_steps(h, 5, nsteps, step_rk4_cfg);
   if (h && h->precision == 1) return run_steps(h, 4, nsteps, step_rk4_mixed);
   return run_steps(h, 3, nsteps, step_rk4);
 }
 
+int kg_set_scheme(kg_solver* h, int scheme, double ko_eps) {
+  if (!h || scheme < 0 || scheme > 1 || !(ko_eps >= 0.0)) return KG_EINVAL;
+  if (scheme == 1 && h->p.metric != KG_KERR_SCHILD)
+    return set_err(h, KG_EINVAL, "the configured method is written for the Kerr_Schild metric form");
+  if (scheme == 1 && h->precision == 1)
+    return set_err(h, KG_EINVAL, "the configured method runs in FP64 (set precision 0 first)");
+  h->scheme = scheme;
+  h->ko_eps = ko_eps;
+  h->graph_gen++;
+  return KG_OK;
+}
+
+int kg_get_scheme(const kg_solver* h) { return h ? h->scheme : -1; }
+
+int kg_fill_ghosts_cfg(kg_solver* h) {
+  if (!h) return KG_EINVAL;
+  kg::launch_ghost_fill_cfg(h->g, h->U, h->stream);
+  KG_CK(cudaGetLastError());
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_OK;
+}
+
 int kg_set_precision(kg_solver* h, int mode) {
   if (!h || mode < 0 || mode > 1) return KG_EINVAL;
+  if (mode == 1 && h->scheme == 1) return set_err(h, KG_EINVAL, "the configured method runs in FP64");
   if (mode == 1 && !kg::tma_available(h->g, h->U)) return set_err(h, KG_EINVAL, "tensor maps unavailable");
   h->precision = mode;
   return KG_OK;

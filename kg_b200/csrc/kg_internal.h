@@ -82,6 +82,12 @@ size_t ghost_f32_desc_bytes();
 void fill_ghost_f32_desc(void* dst, const Grid& g, float2* u, const double2* up, int inflow);
 void launch_ghost_fill_f32(const void* d_desc, int n, long long max_rows, long long max_faces, long long max_z,
                            cudaStream_t st);
+// configured method (kg_config.cu): RK4 stage with fourth-order differences,
+// Kreiss-Oliger dissipation and a Sommerfeld outer plane; coef = 1/(12 h) for
+// r, theta, phi then eps/(64 h) for r, theta, phi; rN = outermost r
+int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, const double coef[6], double rN,
+                     cudaStream_t st);
+void launch_ghost_fill_cfg(const Grid& g, double2* u, cudaStream_t st);
 void launch_rhs(const Grid& g, const Metric& m, int metric_kind, const double2* const in[5], double2* out,
                 unsigned mask, cudaStream_t st);
 

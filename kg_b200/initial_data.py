@@ -12,6 +12,12 @@ the device solver and the CPU oracle:
   c_lm Y_lm(theta, phi) with c_lm complex N(0, sd^2) drawn from a numpy seed,
   Pi = 0 (the Gaussian shell form of main/initial_conditions.f90:62,158).
 
+* ``smooth_exact``   -- for the configured fourth-order method: phi =
+  amp exp(-((r - r0)/w)^2) times a function that is smooth on the sphere
+  (combinations of Re Y_20, Re Y_21, Re Y_22, or Y_20 alone), with psi_1..3 the
+  exact derivatives (so the data carry no second-order differencing error),
+  Pi = 0.
+
 Arrays returned have C shape (NK, NJ, NI, 5), i.e. the Fortran array
 u(1:5, -g:Nx+g, -g:Ny+g, 0:Nz) with the variable index fastest.
 """
@@ -79,6 +85,33 @@ def _assemble(phi, dx, dy, dz, Nz):
     u[..., 2] = _dx2(phi, dy, Nz)
     u[..., 3] = _dx3(phi, dz)
     u[..., 4] = 0.0
+    return u
+
+
+def smooth_exact(Nx, Ny, Nz, xmin, xmax, amp=1.0, r0=10.0, width=2.0, angular="mix"):
+    """phi = amp exp(-((r-r0)/w)^2) f(theta, phi) with exact psi_1..3 and Pi = 0.
+    angular: 'mix' = (3 cos^2 - 1) + 0.5 sin cos cos(phi) + 0.3 sin^2 cos(2 phi);
+    'y20' = sqrt(5/(16 pi)) (3 cos^2 - 1)."""
+    x, y, z, dx, dy, dz = grid_axes(Nx, Ny, Nz, xmin, xmax)
+    T, P = y[None, :, None], z[:, None, None]
+    X = x[None, None, :]
+    c, sn = np.cos(T), np.sin(T)
+    if angular == "y20":
+        a = math.sqrt(5.0 / (16.0 * math.pi))
+        f = a * (3 * c ** 2 - 1) + 0 * P
+        ft = a * (-6 * c * sn) + 0 * P
+        fp = 0 * f
+    else:
+        f = (3 * c ** 2 - 1) + 0.5 * sn * c * np.cos(P) + 0.3 * sn ** 2 * np.cos(2 * P)
+        ft = -6 * c * sn + 0.5 * np.cos(2 * T) * np.cos(P) + 0.6 * sn * c * np.cos(2 * P)
+        fp = -0.5 * sn * c * np.sin(P) - 0.6 * sn ** 2 * np.sin(2 * P)
+    g = amp * np.exp(-((X - r0) / width) ** 2)
+    gr = -2.0 * (X - r0) / width ** 2 * g
+    u = np.zeros((Nz + 1, Ny + 5, Nx + 5, 5), np.complex128)
+    u[..., 0] = f * g
+    u[..., 1] = f * gr
+    u[..., 2] = ft * g
+    u[..., 3] = fp * g
     return u
 
 

@@ -145,6 +145,18 @@ class LinesMethod:
             raise ValueError("precision is 'fp64' or 'mixed'")
         self._ck(self._lib.kg_set_precision(self._h, 1 if mode == "mixed" else 0))
 
+    def set_scheme(self, scheme, ko_eps=0.02):
+        """'reference' (second order, default) or 'configured' (fourth-order
+        differences, sixth-order Kreiss-Oliger dissipation of strength ko_eps,
+        Sommerfeld outer plane, parity-correct pole ghosts; rk4 only)"""
+        if scheme not in ("reference", "configured"):
+            raise ValueError("scheme is 'reference' or 'configured'")
+        self._ck(self._lib.kg_set_scheme(self._h, 0 if scheme == "reference" else 1, float(ko_eps)))
+
+    def fill_ghosts_configured(self):
+        """apply the configured method's ghost fills to u"""
+        self._ck(self._lib.kg_fill_ghosts_cfg(self._h))
+
     def synchronize(self):
         """Wait for the handle's queued device work (steppers return asynchronously)."""
         self._ck(self._lib.kg_synchronize(self._h))

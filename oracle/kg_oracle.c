@@ -84,6 +84,9 @@ typedef struct kgo {
   cplx *tmp[6];
   /* detectors */
   double *r_det; int *index_det;
+  /* scheme: 0 = the reference's second-order method, 1 = configured method */
+  int scheme; double ko_eps;
+  double *dx_beta4;          /* d_r beta^r by the fourth-order stencil (scheme 1) */
 } kgo;
 
 /* ------------------------------------------------------------------ */
@@ -595,7 +598,9 @@ void kgo_rk3(kgo *s, int nsteps) {
   }
 }
 
+static void rk4_cfg(kgo *s, int nsteps);
 void kgo_rk4(kgo *s, int nsteps) {
+  if (s->scheme == 1) { rk4_cfg(s, nsteps); return; }
   const double dt = s->dt;
   for (int step = 0; step < nsteps; ++step) {
     copy_state(s, s->u_p, s->u);
@@ -617,6 +622,234 @@ void kgo_rk4(kgo *s, int nsteps) {
     s->t = s->t + dt;
   }
 }
+
+/* ------------------------------------------------------------------ */
+/* configured method (scheme 1): not in the reference, which wires only
+ * second-order operators (its fourth-order x stencil, first_derivative_x_4 in
+ * tools/finite_differences.f90:124-154, is real-only and never called).
+ *   - first derivatives: the centred fourth-order stencil of
+ *     first_derivative_x_4, (f(i-2) - 8 f(i-1) + 8 f(i+1) - f(i+2)) / (12 h), on
+ *     complex data; in r its one-sided closures at the two first and two last
+ *     stored planes; in theta on the interior rows, whose +-2 neighbours are
+ *     ghost rows; in phi periodic over the Nz-1 distinct planes.  The shift
+ *     advection term uses the same centred operator.
+ *   - sixth-order Kreiss-Oliger dissipation on all five variables,
+ *     + eps / (64 h) (f(-3) - 6 f(-2) + 15 f(-1) - 20 f(0) + 15 f(1) - 6 f(2) + f(3))
+ *     per direction, in r where the stencil fits (planes 3..N-3).
+ *   - Sommerfeld condition at the outermost r plane: d_t u = -(d_r u + u / r).
+ *   - the innermost r planes (inside the horizon) evolve with the one-sided
+ *     closures; no extrapolation.
+ *   - ghost fills: the duplicated phi planes, then the theta ghost rows from
+ *     the interior rows at phi + pi with the parity of a smooth function on the
+ *     sphere (psi_2 = d_theta phi changes sign, the others do not); the theta
+ *     flux alpha sqrt(gamma) gamma^thth psi_2 takes the sign of sin(theta) on
+ *     the ghost rows.
+ * RK4 only; Kerr-Schild metric form only.  Operation order is fixed so the GPU
+ * restatement can match it bit for bit. */
+static inline cplx d4_r(const kgo *s, cplx (*F)(const kgo *, cplx *const *, int, int, int, int), cplx *const *v,
+                        int w, int i, int j, int k, double res) {
+  const int a = s->iL, n = s->iR;
+  cplx r;
+  if (i == a)
+    r = csub(cadd(csub(cadd(rmul(-25.0, F(s, v, w, a, j, k)), rmul(48.0, F(s, v, w, a + 1, j, k))),
+                       rmul(36.0, F(s, v, w, a + 2, j, k))), rmul(16.0, F(s, v, w, a + 3, j, k))),
+             rmul(3.0, F(s, v, w, a + 4, j, k)));
+  else if (i == a + 1)
+    r = cadd(csub(cadd(csub(rmul(-3.0, F(s, v, w, a, j, k)), rmul(10.0, F(s, v, w, a + 1, j, k))),
+                       rmul(18.0, F(s, v, w, a + 2, j, k))), rmul(6.0, F(s, v, w, a + 3, j, k))),
+             rmul(1.0, F(s, v, w, a + 4, j, k)));
+  else if (i == n - 1)
+    r = csub(cadd(csub(cadd(rmul(3.0, F(s, v, w, n, j, k)), rmul(10.0, F(s, v, w, n - 1, j, k))),
+                       rmul(18.0, F(s, v, w, n - 2, j, k))), rmul(6.0, F(s, v, w, n - 3, j, k))),
+             rmul(1.0, F(s, v, w, n - 4, j, k)));
+  else if (i == n)
+    r = cadd(csub(cadd(csub(rmul(25.0, F(s, v, w, n, j, k)), rmul(48.0, F(s, v, w, n - 1, j, k))),
+                       rmul(36.0, F(s, v, w, n - 2, j, k))), rmul(16.0, F(s, v, w, n - 3, j, k))),
+             rmul(3.0, F(s, v, w, n - 4, j, k)));
+  else
+    r = csub(cadd(csub(F(s, v, w, i - 2, j, k), rmul(8.0, F(s, v, w, i - 1, j, k))), rmul(8.0, F(s, v, w, i + 1, j, k))),
+             F(s, v, w, i + 2, j, k));
+  return cmulr(r, res);
+}
+static inline int kper(const kgo *s, int k, int d) {
+  const int M = s->kR - 1; /* Nz - 1 distinct planes 1..Nz-1 */
+  int kk = (k - 1 + d) % M;
+  if (kk < 0) kk += M;
+  return kk + 1;
+}
+static inline cplx d4_c(cplx fm2, cplx fm1, cplx fp1, cplx fp2, double res) {
+  return cmulr(csub(cadd(csub(fm2, rmul(8.0, fm1)), rmul(8.0, fp1)), fp2), res);
+}
+static inline cplx ko6(cplx m3, cplx m2, cplx m1, cplx c0, cplx p1, cplx p2, cplx p3) {
+  return cadd(csub(cadd(csub(cadd(csub(m3, rmul(6.0, m2)), rmul(15.0, m1)), rmul(20.0, c0)), rmul(15.0, p1)),
+                   rmul(6.0, p2)), p3);
+}
+/* point functions of the configured RHS */
+static cplx cf_A(const kgo *s, cplx *const *v, int w, int i, int j, int k) {
+  (void)w;
+  return rmul(s->alpha[P2(s, i, j)], v[4][P3(s, i, j, k)]);
+}
+static cplx cf_E(const kgo *s, cplx *const *v, int w, int i, int j, int k) {
+  (void)w;
+  size_t q = P2(s, i, j), p = P3(s, i, j, k);
+  return cadd(rmul(s->alpha[q], v[4][p]), rmul(s->beta[0][q], v[1][p]));
+}
+static cplx cf_G1(const kgo *s, cplx *const *v, int w, int i, int j, int k) {
+  (void)w;
+  size_t q = P2(s, i, j), p = P3(s, i, j, k);
+  return rmul(s->alpha[q] * s->sqrtg[q], cadd(rmul(s->gamma_up[0][0][q], v[1][p]), rmul(s->gamma_up[0][2][q], v[3][p])));
+}
+/* alpha sqrt(gamma) gamma^thth psi_2: sqrt(gamma) ~ r^2 sin(theta) continues
+ * through the pole with the sign of sin(theta), so on the ghost rows (theta < 0
+ * or > pi, where the table holds |sqrt(gamma)|) the product is negated; with
+ * psi_2 odd the flux is then even and smooth across the pole */
+static cplx cf_H(const kgo *s, cplx *const *v, int w, int i, int j, int k) {
+  (void)w;
+  size_t q = P2(s, i, j);
+  cplx h = rmul(s->alpha[q] * s->sqrtg[q] * s->gamma_up[1][1][q], v[2][P3(s, i, j, k)]);
+  return (j <= 0 || j >= s->Ny) ? cneg(h) : h;
+}
+static cplx cf_Fp(const kgo *s, cplx *const *v, int w, int i, int j, int k) {
+  (void)w;
+  size_t q = P2(s, i, j), p = P3(s, i, j, k);
+  return rmul(s->alpha[q] * s->sqrtg[q], cadd(rmul(s->gamma_up[0][2][q], v[1][p]), rmul(s->gamma_up[2][2][q], v[3][p])));
+}
+static cplx cf_Q(const kgo *s, cplx *const *v, int w, int i, int j, int k) {
+  (void)w;
+  return cmulr(v[4][P3(s, i, j, k)], s->sqrtg[P2(s, i, j)]);
+}
+static cplx cf_P1(const kgo *s, cplx *const *v, int w, int i, int j, int k) {
+  (void)w; return v[1][P3(s, i, j, k)]; }
+static cplx cf_V(const kgo *s, cplx *const *v, int w, int i, int j, int k) { return v[w][P3(s, i, j, k)]; }
+
+/* the configured RHS of all five variables at every stored point */
+static void rhs_cfg(kgo *s, cplx *const *v) {
+  const double rr = 1.0 / (12.0 * s->dx), rt = 1.0 / (12.0 * s->dy), rp = 1.0 / (12.0 * s->dz);
+  const double kr = s->ko_eps / (64.0 * s->dx), kt = s->ko_eps / (64.0 * s->dy), kp = s->ko_eps / (64.0 * s->dz);
+  const double m2 = s->p.m * s->p.m;
+  const int n = s->iR;
+  const double rN = s->x1d[s->iR - s->iL];
+  const cplx z0 = {0.0, 0.0};
+  OMP_K
+  for (int k = s->kL; k <= s->kR; ++k) for (int j = s->jL; j <= s->jR; ++j) for (int i = s->iL; i <= s->iR; ++i) {
+    size_t p = P3(s, i, j, k), q = P2(s, i, j);
+    if (j <= 0 || j >= s->Ny || k == s->kL || k == s->kR) {
+      for (int w = 0; w < 5; ++w) s->rhs_u[w][p] = z0;
+      continue;
+    }
+    if (i == n) { /* Sommerfeld */
+      for (int w = 0; w < 5; ++w)
+        s->rhs_u[w][p] = cneg(cadd(d4_r(s, cf_V, v, w, i, j, k, rr), cdivr(v[w][p], rN)));
+      continue;
+    }
+    const double al = s->alpha[q], b1 = s->beta[0][q], sg = s->sqrtg[q], dxb = s->dx_beta4[q];
+    const int km2 = kper(s, k, -2), km1 = kper(s, k, -1), kp1 = kper(s, k, 1), kp2 = kper(s, k, 2);
+    cplx r[5];
+    r[0] = cadd(rmul(al, v[4][p]), rmul(b1, v[1][p]));
+    r[1] = cadd(cadd(d4_r(s, cf_A, v, 0, i, j, k, rr), rmul(b1, d4_r(s, cf_P1, v, 0, i, j, k, rr))), rmul(dxb, v[1][p]));
+    r[2] = d4_c(cf_E(s, v, 0, i, j - 2, k), cf_E(s, v, 0, i, j - 1, k), cf_E(s, v, 0, i, j + 1, k), cf_E(s, v, 0, i, j + 2, k), rt);
+    r[3] = d4_c(cf_E(s, v, 0, i, j, km2), cf_E(s, v, 0, i, j, km1), cf_E(s, v, 0, i, j, kp1), cf_E(s, v, 0, i, j, kp2), rp);
+    {
+      cplx t1 = cdivr(d4_r(s, cf_G1, v, 0, i, j, k, rr), sg);
+      cplx t2 = cdivr(d4_c(cf_H(s, v, 0, i, j - 2, k), cf_H(s, v, 0, i, j - 1, k), cf_H(s, v, 0, i, j + 1, k),
+                           cf_H(s, v, 0, i, j + 2, k), rt), sg);
+      cplx t3 = cdivr(d4_c(cf_Fp(s, v, 0, i, j, km2), cf_Fp(s, v, 0, i, j, km1), cf_Fp(s, v, 0, i, j, kp1),
+                           cf_Fp(s, v, 0, i, j, kp2), rp), sg);
+      cplx t4 = cmulr(v[4][p], dxb);
+      cplx t5 = cdivr(rmul(b1, d4_r(s, cf_Q, v, 0, i, j, k, rr)), sg);
+      cplx t6 = rmul(al * m2, v[0][p]);
+      r[4] = csub(cadd(cadd(cadd(cadd(t1, t2), t3), t4), t5), t6);
+    }
+    const int km3 = kper(s, k, -3), kp3 = kper(s, k, 3);
+    for (int w = 0; w < 5; ++w) {
+      cplx *u = v[w];
+      cplx a = r[w];
+      if (i >= s->iL + 3 && i <= n - 3)
+        a = cadd(a, rmul(kr, ko6(u[P3(s, i - 3, j, k)], u[P3(s, i - 2, j, k)], u[P3(s, i - 1, j, k)], u[p],
+                                 u[P3(s, i + 1, j, k)], u[P3(s, i + 2, j, k)], u[P3(s, i + 3, j, k)])));
+      a = cadd(a, rmul(kt, ko6(u[P3(s, i, j - 3, k)], u[P3(s, i, j - 2, k)], u[P3(s, i, j - 1, k)], u[p],
+                               u[P3(s, i, j + 1, k)], u[P3(s, i, j + 2, k)], u[P3(s, i, j + 3, k)])));
+      a = cadd(a, rmul(kp, ko6(u[P3(s, i, j, km3)], u[P3(s, i, j, km2)], u[P3(s, i, j, km1)], u[p],
+                               u[P3(s, i, j, kp1)], u[P3(s, i, j, kp2)], u[P3(s, i, j, kp3)])));
+      s->rhs_u[w][p] = a;
+    }
+  }
+}
+
+/* ghost fills of the configured method: duplicated phi planes, then the theta
+ * ghost rows (three per pole) from interior rows at phi + pi, psi_2 negated */
+static void boundary_cfg(kgo *s) {
+  const int NZ = s->kR;
+  for (int w = 0; w < 5; ++w)
+    for (int j = s->jL; j <= s->jR; ++j) for (int i = s->iL; i <= s->iR; ++i) {
+      s->u[w][P3(s, i, j, 0)] = s->u[w][P3(s, i, j, NZ - 1)];
+      s->u[w][P3(s, i, j, NZ)] = s->u[w][P3(s, i, j, 1)];
+    }
+  const int dis = NZ / 2;
+  for (int k = s->kL; k <= s->kR; ++k) {
+    const int kt = (k + dis) % (NZ - 1);
+    for (int g = s->g; g >= 0; --g)
+      for (int w = 0; w < 5; ++w) {
+        const double sgn = (w == 2) ? -1.0 : 1.0;
+        for (int i = s->iL; i <= s->iR; ++i) {
+          s->u[w][P3(s, i, 0 - g, k)] = rmul(sgn, s->u[w][P3(s, i, 0 + g + 1, kt)]);
+          s->u[w][P3(s, i, s->Ny + g, k)] = rmul(sgn, s->u[w][P3(s, i, s->Ny - g - 1, kt)]);
+        }
+      }
+  }
+}
+
+static void rk4_cfg(kgo *s, int nsteps) {
+  const double dt = s->dt;
+  for (int step = 0; step < nsteps; ++step) {
+    copy_state(s, s->u_p, s->u);
+    for (int rk = 1; rk <= 4; ++rk) {
+      rhs_cfg(s, s->u);
+      for (int v = 0; v < 5; ++v) {
+        cplx *u = s->u[v], *up = s->u_p[v], *r = s->rhs_u[v];
+        cplx *k1 = s->k1[v], *k2 = s->k2[v], *k3 = s->k3[v], *k4 = s->k4[v];
+        for (long p = 0; p < (long)s->npts; ++p) {
+          if (rk == 1) { k1[p] = cmulr(r[p], dt); u[p] = cadd(up[p], rmul(0.50, k1[p])); }
+          else if (rk == 2) { k2[p] = cmulr(r[p], dt); u[p] = cadd(up[p], rmul(0.50, k2[p])); }
+          else if (rk == 3) { k3[p] = cmulr(r[p], dt); u[p] = cadd(up[p], k3[p]); }
+          else { k4[p] = cmulr(r[p], dt);
+            u[p] = cadd(up[p], cdivr(cadd(cadd(cadd(k1[p], rmul(2.0, k2[p])), rmul(2.0, k3[p])), k4[p]), 6.0)); }
+        }
+      }
+      boundary_cfg(s);
+    }
+    s->t = s->t + dt;
+  }
+}
+
+/* 0: the reference's second-order method; 1: the configured method above
+ * (RK4 only, Kerr-Schild form); returns 0 or -1 */
+int kgo_set_scheme(kgo *s, int scheme, double ko_eps) {
+  if (scheme < 0 || scheme > 1) return -1;
+  if (scheme == 1 && s->p.metric != KGO_KERR_SCHILD) return -1;
+  if (scheme == 1 && !s->dx_beta4) {
+    /* first_derivative_x_4 (tools/finite_differences.f90:124-154) of beta^r; the
+     * second-order dx_beta of the reference would cap the method at second order */
+    s->dx_beta4 = xcalloc((size_t)s->NI * s->NJ, sizeof(double));
+    const double res = 1.0 / (12.0 * s->dx);
+    const int n = s->iR - s->iL;
+    for (int j = s->jL; j <= s->jR; ++j) {
+      const double *F = s->beta[0] + P2(s, s->iL, j);
+      double *D = s->dx_beta4 + P2(s, s->iL, j);
+      D[0] = (-25.0 * F[0] + 48.0 * F[1] - 36.0 * F[2] + 16.0 * F[3] - 3.0 * F[4]) * res;
+      D[1] = (-3.0 * F[0] - 10.0 * F[1] + 18.0 * F[2] - 6.0 * F[3] + 1.0 * F[4]) * res;
+      for (int o = 2; o <= n - 2; ++o) D[o] = (F[o - 2] - 8.0 * F[o - 1] + 8.0 * F[o + 1] - F[o + 2]) * res;
+      D[n - 1] = (3.0 * F[n] + 10.0 * F[n - 1] - 18.0 * F[n - 2] + 6.0 * F[n - 3] - 1.0 * F[n - 4]) * res;
+      D[n] = (25.0 * F[n] - 48.0 * F[n - 1] + 36.0 * F[n - 2] - 16.0 * F[n - 3] + 3.0 * F[n - 4]) * res;
+    }
+  }
+  s->scheme = scheme;
+  s->ko_eps = ko_eps;
+  return 0;
+}
+
+/* the configured ghost fills on the current state (initial data) */
+void kgo_boundary_cfg(kgo *s) { boundary_cfg(s); }
 
 /* ------------------------------------------------------------------ */
 /* diagnostics                                                         */
@@ -1066,7 +1299,7 @@ void kgo_destroy(kgo *s) {
   }
   for (int t = 0; t < 6; ++t) free(s->tmp[t]);
   for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) { free(s->g_dn[a][b]); free(s->g_up[a][b]); }
-  free(s->alpha); free(s->sqrtg); free(s->dx_beta);
+  free(s->alpha); free(s->sqrtg); free(s->dx_beta); free(s->dx_beta4);
   for (int a = 0; a < 3; ++a) { free(s->beta[a]); for (int b = 0; b < 3; ++b) free(s->gamma_up[a][b]); }
   free(s->x1d); free(s->y1d); free(s->r_det); free(s->index_det);
   free(s);

@@ -66,6 +66,9 @@ def lib():
         L.kgo_currents_detectors.argtypes = [P, D]
         L.kgo_proyector_detectors.argtypes = [P, I, D]
         L.kgo_project_all_shells.argtypes = [P, I, D]
+        L.kgo_set_scheme.argtypes = [P, I, C.c_double]
+        L.kgo_set_scheme.restype = I
+        L.kgo_boundary_cfg.argtypes = [P]
         L.kgo_sph_jl.argtypes = [I, C.c_double]
         L.kgo_sph_jl.restype = C.c_double
         L.kgo_sph_jl_zeros.argtypes = [I, I, D]
@@ -214,6 +217,16 @@ class Oracle:
         out = np.zeros((self.Nx, 2 * L + 1, L + 1), np.complex128)
         lib().kgo_project_all_shells(self.h, L, _dp(out.view(np.float64)))
         return out
+
+    def set_scheme(self, scheme, ko_eps=0.02):
+        """0: the reference's second-order method; 1: the configured fourth-order
+        method with sixth-order Kreiss-Oliger dissipation and a Sommerfeld outer
+        boundary (RK4 only)"""
+        if lib().kgo_set_scheme(self.h, int(scheme), float(ko_eps)) != 0:
+            raise ValueError("scheme 1 needs the Kerr-Schild metric form")
+
+    def boundary_cfg(self):
+        lib().kgo_boundary_cfg(self.h)
 
     def bessel_basis(self, L, Nk):
         """(k_values (Nk, L+1), j_basis (Nx, Nk, L+1))"""
