@@ -236,6 +236,28 @@ int kg_batch_get_tuning(const kg_batch *b, int *kchunk, int *blocks);
 long long kg_batch_launch_count(const kg_batch *b);
 void *kg_batch_get_stream(const kg_batch *b);
 
+/* --- Berger-Oliger refinement ------------------------------------------------ */
+
+/* A hierarchy of radially nested 2:1 levels (the reference's
+ * mesh_refinement_memory/boundary/create, MoL/mesh_refinement_lib.f90:76-179,
+ * build one uniform level; the nesting is new).  Level 0 is kg_create(base);
+ * level l = 1..nlevels-1 covers [xmin, ~r_fine[l-1]] with dx_0 / 2^l and takes
+ * dt_0 / 2^l steps, same theta/phi grid.  Per coarse RK4 step each finer level
+ * steps twice per parent step; after every stage its 4 outermost planes take
+ * the parent's values (cubic in r, linear in time between the parent's states
+ * at its step's start and end); after its two steps it is injected onto the
+ * parent except for its last 8 planes.  Levels are ordinary solver handles
+ * (kg_hier_level) for state access and diagnostics; they belong to the
+ * hierarchy (kg_hier_destroy frees them). */
+typedef struct kg_hier kg_hier;
+int kg_hier_create(const kg_params *base, int nlevels, const double *r_fine, int device, kg_hier **out);
+int kg_hier_destroy(kg_hier *H);
+const char *kg_hier_last_error(const kg_hier *H);
+int kg_hier_levels(const kg_hier *H);
+kg_solver *kg_hier_level(kg_hier *H, int level);
+int kg_hier_rk4(kg_hier *H, int coarse_steps);
+int kg_hier_synchronize(kg_hier *H);
+
 /* --- allocation-free diagnostic --------------------------------------------- */
 
 /* Mass_scalar = integrate(rho*sqrtg) without allocating anything.  No

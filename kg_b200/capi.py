@@ -99,6 +99,13 @@ SIGNATURES = [
     ("kg_batch_synchronize", _I, [_P]),
     ("kg_batch_set_tuning", _I, [_P, _I, _I]),
     ("kg_batch_set_precision", _I, [_P, _I]),
+    ("kg_hier_create", _I, [C.POINTER(KgParams), _I, _D, _I, _PP]),
+    ("kg_hier_destroy", _I, [_P]),
+    ("kg_hier_last_error", C.c_char_p, [_P]),
+    ("kg_hier_levels", _I, [_P]),
+    ("kg_hier_level", _P, [_P, _I]),
+    ("kg_hier_rk4", _I, [_P, _I]),
+    ("kg_hier_synchronize", _I, [_P]),
     ("kg_batch_get_tuning", _I, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("kg_batch_launch_count", C.c_longlong, [_P]),
     ("kg_batch_get_stream", C.c_void_p, [_P]),

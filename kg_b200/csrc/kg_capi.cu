@@ -141,13 +141,14 @@ double2* fld(double2* base, const Grid& g, int v) { return base + (long long)v *
 
 // kernel kinds reported by kg_profile_read: the 13 stage kinds, then these
 enum { PK_GHOST = 13, PK_FACE, PK_RHS, PK_CONVERT, PK_DENSITY, PK_MASS, PK_SHELL, PK_FLUX, PK_PROJECT,
-       PK_YLM_PREP, PK_YLM_GEMM, PK_YLM_FP64, PK_RADIAL, PK_MX1, PK_MX2, PK_MX3, PK_MX4, PK_GHOST_F32, PK_COUNT };
+       PK_YLM_PREP, PK_YLM_GEMM, PK_YLM_FP64, PK_RADIAL, PK_MX1, PK_MX2, PK_MX3, PK_MX4, PK_GHOST_F32, PK_PROLONG,
+       PK_RESTRICT, PK_COUNT };
 const char* const kPkNames[PK_COUNT] = {
     "stage_pirk_s1_psi", "stage_pirk_s1_pi", "stage_pirk2_s2", "stage_pirk3_s2_psi", "stage_pirk3_s2_pi",
     "stage_pirk3_s3", "stage_rk3_1", "stage_rk3_2", "stage_rk3_3", "stage_rk4_1", "stage_rk4_2", "stage_rk4_3",
     "stage_rk4_4", "ghost_fill", "boundary_face", "rhs", "layout_convert", "density", "mass_reduce",
     "shell_interp", "flux_reduce", "ylm_project", "ylm_all_prepare", "ylm_all_gemm_bf16x3", "ylm_all_fp64", "radial_ft", "mixed_rk4_1",
-    "mixed_rk4_2", "mixed_rk4_3", "mixed_rk4_4", "ghost_fill_f32"};
+    "mixed_rk4_2", "mixed_rk4_3", "mixed_rk4_4", "ghost_fill_f32", "bo_prolong", "bo_restrict"};
 
 cudaEvent_t take_event(kg_solver* h) {
   if (!h->pool.empty()) {
@@ -1083,6 +1084,45 @@ int step_rk4_cfg(kg_solver* h, int nsteps) {
   return KG_OK;
 }
 
+// RK4 step of a refined level whose outermost planes follow the coarser level:
+// after every stage the stage output's buffer planes take the coarse values
+// interpolated to the time of the stage that reads them (alpha = position in
+// [t_coarse, t_coarse + dt_coarse]; a0 at this step's start, da its length).
+int step_rk4_bo(kg_solver* h, kg_solver* c, const double2* c_old, double a0, double da, int nbuf) {
+  int rc;
+  if ((rc = ensure(h, &h->RK, 15))) return rc;
+  const Grid& g = h->g;
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  double2* R1 = h->RK;
+  double2* R2 = fld(h->RK, g, 5);
+  double2* A = fld(h->RK, g, 10);
+  auto prolong = [&](double2* u, double alpha) -> int {
+    Prof pf(h, PK_PROLONG, 1);
+    if (kg::launch_prolong(g, u, c->g, c_old, c->U, alpha, nbuf, h->stream))
+      return set_err(h, KG_EINVAL, "refined level does not fit inside its coarser level");
+    return KG_OK;
+  };
+  if ((rc = prolong(h->U, a0))) return rc;
+  kg::StageLaunch L = base_launch(h);
+  L.base = h->U;
+  L.acc = A;
+  double2* ins[4] = {h->U, R1, R2, R1};
+  double2* outs[4] = {R1, R2, R1, h->U};
+  const int kinds[4] = {kg::ST_RK4_1, kg::ST_RK4_2, kg::ST_RK4_3, kg::ST_RK4_4};
+  const double at[4] = {a0 + 0.5 * da, a0 + 0.5 * da, a0 + da, a0 + da};
+  for (int st = 0; st < 4; ++st) {
+    set_in(L, g, ins[st], fld(ins[st], g, 4));
+    L.out = outs[st];
+    L.skip_last_i = (st == 3) ? inflow : 0;
+    run_stage(h, kinds[st], L);
+    run_ghost(h, outs[st], h->U, inflow);
+    if ((rc = prolong(outs[st], at[st]))) return rc;
+  }
+  h->t = h->t + h->dt;
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
 // Runs nsteps steps.  Pairs of steps are replayed from a CUDA graph captured
 // once per stepper and Pi-slot state (two steps return the PIRK slots to the
 // state they started in); an odd last step, or runs with profiling on, launch
@@ -1989,3 +2029,168 @@ long long kg_batch_launch_count(const kg_batch* b) { return b ? b->launches : 0;
 void* kg_batch_get_stream(const kg_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 }  // extern "C"
+
+// =============================================================================
+// Berger-Oliger hierarchy: radially nested 2:1 levels (kg_refine.cu), each a
+// full solver handle on [xmin, r_l] with dx_l = dx_0 / 2^l and dt_l = dt_0 / 2^l.
+// One coarse step: level 0 takes an RK4 step; every finer level takes two
+// steps per step of its parent, its outermost planes following the parent in
+// space and time; then it is restricted onto the parent.
+struct kg_hier {
+  std::vector<kg_solver*> lv;
+  std::vector<double2*> uold;  // state of each non-finest level at the start of its current step
+  std::vector<cudaEvent_t> ev;
+  int nbuf = 4, keep_out = 8;
+  long long coarse_steps = 0;
+  std::string err;
+};
+
+namespace {
+int hier_order(kg_hier* H, kg_solver* from, kg_solver* to, int l) {
+  if (cudaEventRecord(H->ev[l], from->stream) != cudaSuccess ||
+      cudaStreamWaitEvent(to->stream, H->ev[l], 0) != cudaSuccess) {
+    H->err = "stream ordering between levels failed";
+    return KG_ECUDA;
+  }
+  return KG_OK;
+}
+
+int hier_step(kg_hier* H, int l, double a0, double da) {
+  kg_solver* h = H->lv[l];
+  const int n = (int)H->lv.size();
+  int rc;
+  if (l + 1 < n) {
+    if (cudaMemcpyAsync(H->uold[l], h->U, 5 * field_bytes(h), cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess) {
+      H->err = "level state copy failed";
+      return KG_ECUDA;
+    }
+  }
+  if (l == 0) rc = step_rk4(h, 1);
+  else rc = step_rk4_bo(h, H->lv[l - 1], H->uold[l - 1], a0, da, H->nbuf);
+  if (rc) {
+    H->err = h->err;
+    return rc;
+  }
+  if (l + 1 < n) {
+    kg_solver* f = H->lv[l + 1];
+    if ((rc = hier_order(H, h, f, l))) return rc;
+    for (int sub = 0; sub < 2; ++sub)
+      if ((rc = hier_step(H, l + 1, 0.5 * sub, 0.5))) return rc;
+    if ((rc = hier_order(H, f, h, l))) return rc;
+    Prof pf(h, PK_RESTRICT, 1);
+    if (kg::launch_restrict(h->g, h->U, f->g, f->U, H->keep_out, h->stream)) {
+      H->err = "restriction does not fit";
+      return KG_EINVAL;
+    }
+  }
+  return KG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int kg_hier_create(const kg_params* base, int nlevels, const double* r_fine, int device, kg_hier** out) {
+  if (!base || !out || nlevels < 1 || nlevels > 8 || (nlevels > 1 && !r_fine)) return KG_EINVAL;
+  *out = nullptr;
+  kg_hier* H = new kg_hier();
+  kg_solver* h0 = nullptr;
+  int rc = kg_create(base, device, &h0);
+  if (rc) {
+    delete H;
+    return rc;
+  }
+  H->lv.push_back(h0);
+  const double dt0 = h0->dt, dx0 = h0->dx;
+  for (int l = 1; l < nlevels; ++l) {
+    kg_params p = *base;
+    const double dxl = dx0 / (double)(1 << l);
+    const int nx = (int)((r_fine[l - 1] - base->xmin) / dxl);
+    kg_solver* parent = H->lv[l - 1];
+    if (nx < 8 || (nx + 2 * p.g_pts + 1 - 1) / 2 + 2 > parent->NI - 1) {
+      H->err = "refined level " + std::to_string(l) + " must lie inside its parent and hold at least 8 cells";
+      kg_hier_destroy(H);
+      return KG_EINVAL;
+    }
+    p.Nx = nx;
+    p.xmax = base->xmin + (double)nx * dxl;
+    p.dt_override = dt0 / (double)(1 << l);
+    p.bc_rmax = KG_OUTFLOW;
+    kg_solver* hl = nullptr;
+    if ((rc = kg_create(&p, device, &hl))) {
+      H->err = "creating refined level failed";
+      kg_hier_destroy(H);
+      return rc;
+    }
+    H->lv.push_back(hl);
+  }
+  for (int l = 0; l + 1 < nlevels; ++l) {
+    double2* b = nullptr;
+    if ((rc = dalloc(H->lv[l], (void**)&b, 5 * field_bytes(H->lv[l])))) {
+      H->err = "allocating level copies failed";
+      kg_hier_destroy(H);
+      return rc;
+    }
+    H->uold.push_back(b);
+  }
+  H->ev.resize(nlevels);
+  for (auto& e : H->ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  *out = H;
+  return KG_OK;
+}
+
+int kg_hier_destroy(kg_hier* H) {
+  if (!H) return KG_EINVAL;
+  for (kg_solver* h : H->lv)
+    if (h) cudaStreamSynchronize(h->stream);
+  for (double2* b : H->uold)
+    if (b) cudaFree(b);
+  for (auto e : H->ev)
+    if (e) cudaEventDestroy(e);
+  for (kg_solver* h : H->lv)
+    if (h) kg_destroy(h);
+  delete H;
+  return KG_OK;
+}
+
+const char* kg_hier_last_error(const kg_hier* H) { return H ? H->err.c_str() : "null hierarchy"; }
+
+int kg_hier_levels(const kg_hier* H) { return H ? (int)H->lv.size() : 0; }
+
+kg_solver* kg_hier_level(kg_hier* H, int l) {
+  return (H && l >= 0 && l < (int)H->lv.size()) ? H->lv[l] : nullptr;
+}
+
+// nsteps coarse steps of RK4 (MoL/lines_method_lib.f90:411-474) on every level
+int kg_hier_rk4(kg_hier* H, int nsteps) {
+  if (!H || nsteps < 0) return KG_EINVAL;
+  for (kg_solver* h : H->lv)
+    if (h->scheme != 0 || h->precision != 0) {
+      H->err = "the hierarchy steps the reference FP64 scheme";
+      return KG_EINVAL;
+    }
+  for (int s = 0; s < nsteps; ++s) {
+    const int rc = hier_step(H, 0, 0.0, 1.0);
+    if (rc) return rc;
+    H->coarse_steps++;
+  }
+  return KG_OK;
+}
+
+int kg_hier_synchronize(kg_hier* H) {
+  if (!H) return KG_EINVAL;
+  for (kg_solver* h : H->lv) {
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+      H->err = "synchronize failed";
+      return KG_ECUDA;
+    }
+    const int rc = check_device_flag(h);
+    if (rc) {
+      H->err = h->err;
+      return rc;
+    }
+  }
+  return KG_OK;
+}
+
+}  // extern "C"
+

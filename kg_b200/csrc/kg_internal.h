@@ -88,6 +88,10 @@ void launch_ghost_fill_f32(const void* d_desc, int n, long long max_rows, long l
 int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, const double coef[6], double rN,
                      cudaStream_t st);
 void launch_ghost_fill_cfg(const Grid& g, double2* u, cudaStream_t st);
+// Berger-Oliger transfers between radially nested 2:1 levels (kg_refine.cu)
+int launch_prolong(const Grid& gf, double2* uf, const Grid& gc, const double2* c_old, const double2* c_new,
+                   double alpha, int nbuf, cudaStream_t st);
+int launch_restrict(const Grid& gc, double2* uc, const Grid& gf, const double2* uf, int keep_out, cudaStream_t st);
 void launch_rhs(const Grid& g, const Metric& m, int metric_kind, const double2* const in[5], double2* out,
                 unsigned mask, cudaStream_t st);
 
