@@ -192,25 +192,24 @@ def _wave(d):
 
 def precision_leg(w, device, steps=40, every=10, L=64):
     """The precision form on the workload grid: RK4 with the FP32 stencil RHS and
-    FP64 state update, a split-BF16 tensor-core Y_lm projection (l <= L, every
-    shell) every `every` steps, against the FP64 RK4 run with the FP64
-    projection, from the same initial data.  Throughput is device time of the
-    steps plus projections; errors are those of the final projection, of the
-    l <= 8 detector waveform at r = 50 over the run, and of phi and Pi."""
+    FP64 state update plus a split-BF16 tensor-core Y_lm projection (l <= L, every
+    shell) every `every` steps, against FP64 RK4 with the FP64 projection, from
+    the same initial data.  Device time (CUDA events) of the steps and of the
+    projections; errors of phi and Pi, of the l <= 8 detector waveforms at
+    r = 12 (inside the shell) and r = 50, and of the last all-shell projection."""
     import torch
     from kg_b200 import ScalarField
     from kg_b200.initial_data import shell_ylm_device
-    out = {}
     runs = {}
     for prec in ("fp64", "mixed"):
         s = ScalarField(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], m=w["m"], device=device,
-                        l_max=8, n_det=1)
+                        l_max=8, n_det=2)
         u0, _ = shell_ylm_device(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], seed=w["seed"],
                                  device=f"cuda:{device}")
         s._ck(s._lib.kg_set_state_device(s.handle, 0, C.c_void_p(u0.data_ptr())))
         s.synchronize()
         del u0
-        s.set_detectors([50.0])
+        s.set_detectors([12.0, 50.0])
         s.precision = prec
         lib, h = s._lib, s.handle
         stream = torch.cuda.ExternalStream(lib.kg_get_stream(h), device=f"cuda:{device}")
@@ -219,41 +218,145 @@ def precision_leg(w, device, steps=40, every=10, L=64):
         s.rk4(nsteps=2)  # warm: buffers, graphs
         s._ck(lib.kg_project_all_shells(h, L, alm_p, host.ctypes.data_as(C.POINTER(C.c_double))))
         s.synchronize()
+        nk = lib.kg_profile_kinds()
+        names = [lib.kg_profile_kind_name(i).decode() for i in range(nk)]
+        pms, pcnt = (C.c_double * nk)(), (C.c_longlong * nk)()
         wave = []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        dev_ms = 0.0
+        step_ms = proj_ms = 0.0
         for q in range(steps // every):
             e0.record(stream)
             s.rk4(nsteps=every)
-            # projection kernels only (the host copy of the coefficients is outside the timed region)
-            s._ck(lib.kg_project_all_shells(h, L, alm_p, host.ctypes.data_as(C.POINTER(C.c_double))))
             e1.record(stream)
             e1.synchronize()
-            dev_ms += e0.elapsed_time(e1)
-            wave.append(s.proyector_detectors()[0].copy())
+            step_ms += e0.elapsed_time(e1)
+            lib.kg_profile_read(h, pms, pcnt)
+            lib.kg_profile_enable(h, 1)
+            s._ck(lib.kg_project_all_shells(h, L, alm_p, host.ctypes.data_as(C.POINTER(C.c_double))))
+            lib.kg_profile_read(h, pms, pcnt)
+            lib.kg_profile_enable(h, 0)
+            proj_ms += sum(pms[i] for i in range(nk) if names[i].startswith("ylm_all"))
+            wave.append(s.proyector_detectors().copy())
         st = torch.empty((w["Nz"] + 1, w["Ny"] + 5, w["Nx"] + 5, 5), dtype=torch.complex128,
                          device=f"cuda:{device}")
         s._ck(lib.kg_get_state_device(h, 0, C.c_void_p(st.data_ptr())))
         s.synchronize()
-        runs[prec] = dict(ms=dev_ms, alm=host.copy(), wave=np.array(wave), phi=st[..., 0].clone(),
-                          pi=st[..., 4].clone())
+        runs[prec] = dict(step_ms=step_ms, proj_ms=proj_ms, alm=host.copy(), wave=np.array(wave),
+                          phi=st[..., 0].clone(), pi=st[..., 4].clone())
         del st
         s.close()
         torch.cuda.empty_cache()
     pts = interior_points(w) * 4 * steps
     a, b = runs["fp64"], runs["mixed"]
-    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
     trel = lambda x, y: float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y))
-    wave_mode = np.linalg.norm(b["wave"] - a["wave"], axis=0) / np.maximum(np.linalg.norm(a["wave"], axis=0), 1e-300)
-    big = np.linalg.norm(a["wave"], axis=0) > 1e-3 * np.linalg.norm(a["wave"], axis=0).max()
-    out = {"workload": f"RK4 on the {w['Nx']}x{w['Ny']}x{w['Nz']} grid, {steps} steps, all-shell Y_lm projection "
-                       f"(l<={L}) every {every} steps; detector at r=50",
-           "fp64_gpsu": pts / (a["ms"] / 1e3), "mixed_gpsu": pts / (b["ms"] / 1e3),
-           "speedup": a["ms"] / b["ms"],
-           "phi_rel_l2_err": trel(b["phi"], a["phi"]), "pi_rel_l2_err": trel(b["pi"], a["pi"]),
-           "waveform_rel_l2_err_l8_r50": rel(b["wave"], a["wave"]),
-           "waveform_max_per_mode_rel_err": float(wave_mode[big].max()) if big.any() else None,
-           "projection_energy_norm_rel_err": rel(b["alm"], a["alm"])}
+
+    def wave_err(d):
+        ref, got = a["wave"][:, d], b["wave"][:, d]
+        n = np.linalg.norm(ref)
+        if n <= 1e-10:
+            return {"rel_l2": None, "ref_norm": float(n), "note": "no signal at this radius within the run"}
+        per_mode = np.linalg.norm(got - ref, axis=0) / np.maximum(np.linalg.norm(ref, axis=0), 1e-300)
+        big = np.linalg.norm(ref, axis=0) > 1e-3 * np.linalg.norm(ref, axis=0).max()
+        return {"rel_l2": float(np.linalg.norm(got - ref) / n), "max_per_mode_rel": float(per_mode[big].max()),
+                "ref_norm": float(n)}
+    return {"workload": f"RK4 on the {w['Nx']}x{w['Ny']}x{w['Nz']} grid, {steps} steps, all-shell Y_lm projection "
+                        f"(l<={L}) every {every} steps; detectors at r = 12 and 50",
+            "fp64_step_gpsu": pts / (a["step_ms"] / 1e3), "mixed_step_gpsu": pts / (b["step_ms"] / 1e3),
+            "step_speedup": a["step_ms"] / b["step_ms"],
+            "fp64_projection_ms": a["proj_ms"] / (steps // every),
+            "tensor_core_projection_ms": b["proj_ms"] / (steps // every),
+            "combined_speedup": (a["step_ms"] + a["proj_ms"]) / (b["step_ms"] + b["proj_ms"]),
+            "phi_rel_l2_err": trel(b["phi"], a["phi"]), "pi_rel_l2_err": trel(b["pi"], a["pi"]),
+            "waveform_r12": wave_err(0), "waveform_r50": wave_err(1),
+            "projection_energy_norm_rel_err": float(np.linalg.norm(b["alm"] - a["alm"]) / np.linalg.norm(a["alm"]))}
+
+
+def c0_leg(device, steps=1000):
+    """The plain FP64 test-field description on the configured method: Nr = 256
+    on [1.8, 60], 32 x 64 theta x phi cells (Nx=256, Ny=33, Nz=65), Kerr-Schild
+    M = 1, m = 0, fourth-order differences, sixth-order Kreiss-Oliger eps = 0.02,
+    Sommerfeld outer plane, RK4, 1000 steps, phi = 1e-3 exp(-(r-10)^2) Y_20 with
+    exact derivatives, Pi = 0.  dt is the reference rule (CFL 0.25); the
+    description's dt = 0.25 dr is also run for 100 steps to record whether it is
+    stable on this grid."""
+    import torch
+    from kg_b200 import ScalarField
+    from kg_b200.initial_data import smooth_exact
+    Nx, Ny, Nz, xmin, xmax = 256, 33, 65, 1.8, 60.0
+    u0 = smooth_exact(Nx, Ny, Nz, xmin, xmax, amp=1e-3, r0=10.0, width=1.0, angular="y20")
+    s = ScalarField(Nx, Ny, Nz, xmin, xmax, 0.25, m=0.0, device=device)
+    s.set_scheme("configured", 0.02)
+    s.u = u0
+    s.fill_ghosts_configured()
+    s.density()
+    m0 = s.mass_scalar()
+    s.rk4(nsteps=2)
+    s.u = u0
+    s.fill_ghosts_configured()
+    s.t = 0.0
+    stream = torch.cuda.ExternalStream(s._lib.kg_get_stream(s.handle), device=f"cuda:{device}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.rk4(nsteps=steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    s.density()
+    m1 = s.mass_scalar()
+    dt = s.dt
+    s.close()
+    t = ScalarField(Nx, Ny, Nz, xmin, xmax, 0.25, m=0.0, device=device, dt=0.25 * (xmax - xmin) / Nx)
+    t.set_scheme("configured", 0.02)
+    t.u = u0
+    t.fill_ghosts_configured()
+    t.rk4(nsteps=100)
+    t.density()
+    m_big = t.mass_scalar()
+    t.close()
+    return {"workload": "Nx=256 Ny=33 Nz=65 on [1.8, 60], configured method (4th-order FD, KO6 0.02, Sommerfeld), "
+                        f"RK4 x{steps}, FP64", "dt": dt, "gpsu": Nx * (Ny - 1) * (Nz - 1) * 4 * steps / (ms / 1e3),
+            "ms_per_step": ms / steps, "mass_start": m0, "mass_end": m1,
+            "dt_0.25dr": {"dt": 0.25 * (xmax - xmin) / Nx, "mass_after_100_steps": m_big,
+                          "stable": bool(np.isfinite(m_big) and abs(m_big) < 1e3 * abs(m0))}}
+
+
+def refinement_leg(w, device, steps=10, r_fine=(20.0, 15.0, 10.0)):
+    """The workload grid as the coarse level of a Berger-Oliger hierarchy with
+    radially nested 2:1 levels inside r < 20 (r_fine), FP64 RK4; level l takes
+    2^l steps per coarse step.  Rate = interior points x 4 stages x steps summed
+    over levels / device time (CUDA events on the coarse level's stream, which
+    every level's work is ordered back into)."""
+    import torch
+    from kg_b200.refinement import BergerOliger
+    from kg_b200.initial_data import shell_ylm_device
+    bo = BergerOliger(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], r_fine=r_fine, m=w["m"],
+                      device=device, l_max=8)
+    for lv in bo.levels:
+        u0, _ = shell_ylm_device(lv.Nx, lv.Ny, lv.Nz, w["xmin"], lv.params.xmax, seed=w["seed"],
+                                 device=f"cuda:{device}")
+        lv._ck(lv._lib.kg_set_state_device(lv.handle, 0, C.c_void_p(u0.data_ptr())))
+        lv.synchronize()
+        del u0
+    bo.rk4(1)
+    bo.synchronize()
+    l0 = bo.levels[0]
+    stream = torch.cuda.ExternalStream(l0._lib.kg_get_stream(l0.handle), device=f"cuda:{device}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    bo.rk4(steps)
+    e1.record(stream)
+    e1.synchronize()
+    bo.synchronize()
+    ms = e0.elapsed_time(e1)
+    work = sum(lv.Nx * (lv.Ny - 1) * (lv.Nz - 1) * 4 * (2 ** l) for l, lv in enumerate(bo.levels)) * steps
+    finite = True
+    for lv in bo.levels:
+        lv.density()
+        finite = finite and bool(np.isfinite(lv.mass_scalar()))
+    out = {"workload": f"coarse level = the workload grid; 2:1 levels inside r < {r_fine}, RK4, {steps} coarse steps",
+           "levels": [{"Nx": lv.Nx, "r_outer": lv.params.xmax, "dt": lv.dt} for lv in bo.levels],
+           "ms_per_coarse_step": ms / steps, "gpsu": work / (ms / 1e3), "finite": finite}
+    bo.close()
     return out
 
 
@@ -370,6 +473,8 @@ def main():
     ap.add_argument("--serve-count", type=int, default=120)
     ap.add_argument("--no-projection", action="store_true", help="skip the all-shell Y_lm projection leg")
     ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision leg")
+    ap.add_argument("--no-refinement", action="store_true", help="skip the Berger-Oliger leg")
+    ap.add_argument("--no-c0", action="store_true", help="skip the configured-method test-field leg")
     args = ap.parse_args()
     if args.grid:
         nx, ny, nz = (int(v) for v in args.grid.split(","))
@@ -511,11 +616,16 @@ def main():
             "gpu_launches": int(launches), "clocks": clk}
     if rank == 0 and world == 1 and not args.no_projection:
         line["projection"] = projection_leg(mol, lib, h)
-    if rank == 0 and world == 1 and not args.grid and not (args.no_precision and args.no_serve):
+    if rank == 0 and world == 1 and not args.grid and not (args.no_precision and args.no_serve and
+                                                            args.no_refinement and args.no_c0):
         mol.close()  # the legs below allocate their own solves
         torch.cuda.empty_cache()
         if not args.no_precision:
             line["precision"] = precision_leg(w, local)
+        if not args.no_refinement:
+            line["refinement"] = refinement_leg(w, local)
+        if not args.no_c0:
+            line["c0_configured"] = c0_leg(local)
         if not args.no_serve:
             line["serving"] = serve_leg(args.serve_count, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
