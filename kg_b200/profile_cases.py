@@ -1,0 +1,90 @@
+"""Small, self-contained runs of each kernel family, for profilers.
+
+    python -m kg_b200.profile_cases mixed      [--grid Nx,Ny,Nz] [--steps K]
+    python -m kg_b200.profile_cases configured [--grid Nx,Ny,Nz] [--steps K]
+    python -m kg_b200.profile_cases batch      [--solves N] [--precision fp64|mixed] [--steps K]
+    python -m kg_b200.profile_cases refine     [--grid Nx,Ny,Nz] [--steps K]
+
+Each case builds seeded synthetic input on the device, runs K steps and exits
+0 (or raises); the sizes default to a few GB of device memory, larger than
+L2, so a profiler capture of one launch is representative and ends quickly.
+  mixed:      RK4 with the FP32 stencil RHS and FP64 update (mixed_rk4_* kernels)
+  configured: RK4 of the fourth-order method (cfg_stage_kernel)
+  batch:      the serving request mix advanced as one batch (tma_batch_kernel /
+              mx_batch_kernel, persistent over a ragged work list)
+  refine:     a two-level Berger-Oliger hierarchy (prolong/restrict kernels)
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import sys
+
+
+def _grid(s, default):
+    return tuple(int(v) for v in s.split(",")) if s else default
+
+
+def _device_ic(s, Nx, Ny, Nz, xmin, xmax, seed=7):
+    from .initial_data import shell_ylm_device
+    u0, _ = shell_ylm_device(Nx, Ny, Nz, xmin, xmax, seed=seed, device="cuda:0")
+    s._ck(s._lib.kg_set_state_device(s.handle, 0, C.c_void_p(u0.data_ptr())))
+    s.synchronize()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["mixed", "configured", "batch", "refine"])
+    ap.add_argument("--grid", default=None)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--solves", type=int, default=30)
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    a = ap.parse_args(argv)
+    from .lines_method import ScalarField
+    if a.case == "mixed":
+        Nx, Ny, Nz = _grid(a.grid, (384, 129, 257))
+        xmax = 1.8 + 0.1944 * Nx
+        s = ScalarField(Nx, Ny, Nz, 1.8, xmax, 0.25, m=0.3, device=0)
+        _device_ic(s, Nx, Ny, Nz, 1.8, xmax)
+        s.precision = "mixed"
+        for _ in range(a.steps):
+            s.rk4(nsteps=1)
+        s.synchronize()
+    elif a.case == "configured":
+        from .initial_data import smooth_exact
+        Nx, Ny, Nz = _grid(a.grid, (384, 65, 129))
+        s = ScalarField(Nx, Ny, Nz, 1.8, 60.0, 0.25, m=0.0, device=0)
+        s.set_scheme("configured", 0.02)
+        s.u = smooth_exact(Nx, Ny, Nz, 1.8, 60.0, amp=1e-3, r0=10.0, width=1.0, angular="y20")
+        s.fill_ghosts_configured()
+        for _ in range(a.steps):
+            s.rk4(nsteps=1)
+        s.synchronize()
+    elif a.case == "batch":
+        from .batch import Batch
+        from .serve import draw_requests, _make_solve
+        reqs = draw_requests(seed=20240602, rate=2000.0, count=a.solves, nr=(128, 512), nr_step=64,
+                             ntheta=(16, 32), steps=(100, 1000), quantum=10)
+        b = Batch(0, precision=a.precision)
+        b.set_tuning(64, 296)
+        solves = [_make_solve(r, 8, 0) for r in reqs]
+        for s in solves:
+            b.add(s)
+        for _ in range(a.steps):
+            b.rk4(1)
+        b.synchronize()
+    else:
+        from .refinement import BergerOliger
+        Nx, Ny, Nz = _grid(a.grid, (512, 65, 129))
+        xmax = 1.8 + 0.1944 * Nx
+        bo = BergerOliger(Nx, Ny, Nz, 1.8, xmax, 0.25, r_fine=(20.0,), m=0.3, device=0)
+        for lv in bo.levels:
+            _device_ic(lv, lv.Nx, lv.Ny, lv.Nz, 1.8, lv.params.xmax)
+        bo.rk4(a.steps)
+        bo.synchronize()
+    print("ok", a.case)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
