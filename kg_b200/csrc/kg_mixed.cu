@@ -45,10 +45,24 @@ __host__ __device__ constexpr int slot_e() {
 }
 constexpr int MW = TI + 2 * RH, MH = TJ + 2, MT_N = MW * MH;
 enum { MT_AL = 0, MT_BE, MT_A, MT_GRR, MT_GRP, MT_SG, MT_HT, MT_COUNT };
+// stages 2-4 (FP32 ring) stage their point-wise operands -- u^n (FP64) and the
+// increment sum (FP32), five variables of the thread's own point -- in shared
+// memory with cp.async issued at the start of each plane, so the loads run
+// under the RHS arithmetic instead of after it
+constexpr int STG_BYTES = TI * TJ * 5 * (16 + 8);
 template <class T>
 __host__ __device__ constexpr size_t mx_smem() {
-  return (size_t)NST * slot_e<T>() * sizeof(T) + (size_t)MT_COUNT * MT_N * 8 + 64 + 128;
+  return (size_t)NST * slot_e<T>() * sizeof(T) + (size_t)MT_COUNT * MT_N * 8 + 64 + 128 +
+         (sizeof(T) == 4 ? (size_t)STG_BYTES : 0);
 }
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(saddr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // ---- a complex value in arithmetic type R -----------------------------------
 template <class R>
@@ -245,7 +259,10 @@ __device__ __forceinline__ void mx_EF(const TIN* st, int tx, int ty, const doubl
 template <int KIND, int MK, class TIN>
 __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMap* tp0p, const CUtensorMap* tp1p,
                                        const MxArgs& a, int bx, int by, int bz, TIN* ring, double* mt,
-                                       uint64_t* bars, uint32_t tb) {
+                                       uint64_t* bars, uint32_t tb, unsigned char* stg) {
+  constexpr bool STG = sizeof(TIN) == 4;
+  double2* base_s = reinterpret_cast<double2*>(stg);
+  float2* acc_s = reinterpret_cast<float2*>(stg + (size_t)TI * TJ * 5 * 16);
   const Grid& g = a.g;
   const Metric& M = a.m;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TI + tx;
@@ -336,6 +353,15 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
       }
       prefetch(k + 2);
     }
+    if (STG && act) {
+      const long long p0 = pcol + (long long)k * g.plane;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        cp_async16(&base_s[v * TI * TJ + tid], a.base + (long long)v * g.fs + p0);
+        cp_async8(&acc_s[v * TI * TJ + tid], a.acc + (long long)v * g.fs + p0);
+      }
+      cp_async_commit();
+    }
     const int tc = i + 1, tn = i + 2;
     const bool okc = mbar_wait_bounded(&bars[slot(tc)], parity(tc));
     const bool okn = okc && mbar_wait_bounded(&bars[slot(tn)], parity(tn));
@@ -361,6 +387,7 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
       const long long p = pcol + (long long)k * g.plane;
       const int n = g.NI - 1;
       const double dt = g.dt;
+      if (STG) cp_async_wait_all();
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
         const long long o = (long long)v * g.fs + p;
@@ -369,6 +396,8 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
         if (KIND == ST_RK4_1) {
           const TIN* e = cu + (size_t)v * FIELD_E + (ty + 1) * RW + 2 * (tx + RH);
           b = make_double2((double)e[0], (double)e[1]);  // the stencil input is u^n itself
+        } else if (STG) {
+          b = base_s[v * TI * TJ + tid];
         } else {
           b = ldf(a.base, o);
         }
@@ -377,13 +406,13 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
           const double2 s = cadd(b, rmul(0.50, kk));
           a.outf[o] = make_float2((float)s.x, (float)s.y);
         } else if (KIND == ST_RK4_2 || KIND == ST_RK4_3) {
-          const float2 av = a.acc[o];
+          const float2 av = STG ? acc_s[v * TI * TJ + tid] : a.acc[o];
           const double2 acc = cadd(make_double2((double)av.x, (double)av.y), rmul(2.0, kk));
           a.acc[o] = make_float2((float)acc.x, (float)acc.y);
           const double2 s = (KIND == ST_RK4_2) ? cadd(b, rmul(0.50, kk)) : cadd(b, kk);
           a.outf[o] = make_float2((float)s.x, (float)s.y);
         } else if (!(a.skip_last_i && ii == n)) {
-          const float2 av = a.acc[o];
+          const float2 av = STG ? acc_s[v * TI * TJ + tid] : a.acc[o];
           a.outd[o] = cadd(b, cdivr(cadd(make_double2((double)av.x, (double)av.y), kk), 6.0));
         }
       }
@@ -394,6 +423,7 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
     }
     failed = __syncthreads_or(timed_out) != 0;
   }
+  if (STG) cp_async_wait_all();  // no staged copy outlives the item
   if (failed) {
     if (tid == 0) {
       atomicExch(a.err, 1);
@@ -433,9 +463,10 @@ __global__ void __launch_bounds__(TI * TJ, 2)
   TIN* ring = reinterpret_cast<TIN*>(align128(smem_raw));
   double* mt = reinterpret_cast<double*>(ring + (size_t)NST * slot_e<TIN>());
   uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
+  unsigned char* stg = reinterpret_cast<unsigned char*>(bars + 8);
   if ((int)blockIdx.z * a.kchunk >= a.g.NK) return;
   init_bars(bars);
-  (void)mx_item<KIND, MK, TIN>(&tin, &tp0, &tp1, a, blockIdx.x, blockIdx.y, blockIdx.z, ring, mt, bars, 0u);
+  (void)mx_item<KIND, MK, TIN>(&tin, &tp0, &tp1, a, blockIdx.x, blockIdx.y, blockIdx.z, ring, mt, bars, 0u, stg);
 }
 
 template <int KIND, int MK, class TIN>
@@ -445,6 +476,7 @@ __global__ void __launch_bounds__(TI * TJ, 2) mx_batch_kernel(const MxItem* __re
   TIN* ring = reinterpret_cast<TIN*>(align128(smem_raw));
   double* mt = reinterpret_cast<double*>(ring + (size_t)NST * slot_e<TIN>());
   uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
+  unsigned char* stg = reinterpret_cast<unsigned char*>(bars + 8);
   __shared__ MxArgs sa;
   __shared__ int s_bx, s_by, s_bz, s_solve;
   init_bars(bars);
@@ -467,7 +499,7 @@ __global__ void __launch_bounds__(TI * TJ, 2) mx_batch_kernel(const MxItem* __re
     }
     __syncthreads();
     const MxItem& B = solves[s_solve];
-    const int used = mx_item<KIND, MK, TIN>(&B.tin, &B.tp0, &B.tp1, sa, s_bx, s_by, s_bz, ring, mt, bars, tb);
+    const int used = mx_item<KIND, MK, TIN>(&B.tin, &B.tp0, &B.tp1, sa, s_bx, s_by, s_bz, ring, mt, bars, tb, stg);
     if (used < 0) break;
     tb += (uint32_t)used;
     __syncthreads();
