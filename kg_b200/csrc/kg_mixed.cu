@@ -269,6 +269,16 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
   const int ii0 = bx * TI, jj0 = by * TJ;
   const int ii = ii0 + tx, jj = jj0 + ty;
   const bool act = (ii < g.NI) && (jj < g.NJ);
+  // ring slot protocol: full[s] completes when a plane's box has landed (one
+  // expect_tx arrival + the bytes); empty[s] when every warp has read the plane
+  // for the last time (one arrival per warp), after which thread 0 may load the
+  // next plane into the slot -- warps are not held at a block barrier per plane
+  uint64_t* empty = bars + NST;
+  const int lane = tid & 31;
+  auto release = [&](int t) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[(tb + (uint32_t)t) % NST]);
+  };
   const int k0 = bz * a.kchunk;
   if (k0 >= g.NK) return 0;
   const int k1 = min(k0 + a.kchunk, g.NK);
@@ -342,14 +352,21 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
   double2 Epv = make_double2(0, 0), Fpv = Epv, Ecu = Epv, Fcu = Epv;
   if (!mbar_wait_bounded(&bars[slot(0)], parity(0))) timed_out = 1;
   if (act && !timed_out) EF(ring + (size_t)slot(0) * slot_e<TIN>(), Epv, Fpv);
+  release(0);
   bool failed = __syncthreads_or(timed_out) != 0;
+  const int last = k1 - k0 - 1;
 
-  for (int i = 0; i < k1 - k0 && !failed; ++i) {
+  for (int i = 0; i <= last && !failed; ++i) {
     const int k = k0 + i;
-    if (tid == 0) {
+    if (tid == 0 && !timed_out) {
       if (i + NST < nplanes) {
-        issue(i + NST);
-        nissued = i + NST + 1;
+        // plane i shares the slot; every warp released it after its last use
+        if (mbar_wait_bounded(&empty[slot(i)], parity(i))) {
+          issue(i + NST);
+          nissued = i + NST + 1;
+        } else {
+          timed_out = 1;
+        }
       }
       prefetch(k + 2);
     }
@@ -363,9 +380,11 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
       cp_async_commit();
     }
     const int tc = i + 1, tn = i + 2;
-    const bool okc = mbar_wait_bounded(&bars[slot(tc)], parity(tc));
-    const bool okn = okc && mbar_wait_bounded(&bars[slot(tn)], parity(tn));
-    if (!okn) timed_out = 1;
+    if (!timed_out) {
+      const bool okc = mbar_wait_bounded(&bars[slot(tc)], parity(tc));
+      const bool okn = okc && mbar_wait_bounded(&bars[slot(tn)], parity(tn));
+      if (!okn) timed_out = 1;
+    }
     if (act && !timed_out) {
       const TIN* cu = ring + (size_t)slot(tc) * slot_e<TIN>();
       const TIN* nx = ring + (size_t)slot(tn) * slot_e<TIN>();
@@ -421,8 +440,10 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
       Ecu = Enx;
       Fcu = Fnx;
     }
-    failed = __syncthreads_or(timed_out) != 0;
+    release(i + 1);
+    if (i == last) release(i + 2);
   }
+  failed = __syncthreads_or(timed_out) != 0;
   if (STG) cp_async_wait_all();  // no staged copy outlives the item
   if (failed) {
     if (tid == 0) {
@@ -448,6 +469,7 @@ __device__ __forceinline__ unsigned char* align128(unsigned char* p) {
 __device__ __forceinline__ void init_bars(uint64_t* bars) {
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[NST + s], TI * TJ / 32);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
