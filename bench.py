@@ -176,13 +176,66 @@ def serve_leg(count, device):
     batched = Server(mode="batched", device=device, tuning=tune).run(reqs)
     mixed = Server(mode="batched", device=device, tuning=tune, precision="mixed").run(reqs)
     strip = lambda d: {k: d[k] for k in ("completed", "wall_s", "solves_per_s", "p50_s", "p99_s") if k in d}
-    return {"workload": SERVE_DESC, "requests": count, "plain_fp64": strip(plain),
+    engine = engine_leg(reqs, device, tune)
+    return {"workload": SERVE_DESC, "requests": count, "engine_device_time": engine, "plain_fp64": strip(plain),
             "batched_fp64": dict(strip(batched), peak_live=batched.get("peak_live"), tuning=list(tune)),
             "batched_mixed": dict(strip(mixed), peak_live=mixed.get("peak_live")),
             "speedup_batched_fp64": batched["solves_per_s"] / plain["solves_per_s"],
             "speedup_batched_mixed": mixed["solves_per_s"] / plain["solves_per_s"],
             "waveform_batched_fp64_vs_plain": _wave(waveform_error_detail(batched, plain)),
             "waveform_batched_mixed_vs_plain_fp64": _wave(waveform_error_detail(mixed, plain))}
+
+
+def engine_leg(reqs, device, tune, steps=10):
+    """Device time (CUDA events, best of 3) of `steps` RK4 steps of every request:
+    one after another on its own handle (plain FP64, graph replay) against all of
+    them in one batch (FP64 and mixed).  Host-side work of the serving loop
+    (request creation, waveform sampling) is outside; the wall-clock serving
+    figures above include it."""
+    import torch
+    from kg_b200.serve import _make_solve
+    from kg_b200.batch import Batch
+    pts = sum((r.Nr + 5) * (r.Ntheta + 6) * (2 * r.Ntheta + 2) for r in reqs)
+    plain_ms = 0.0
+    for r in reqs:
+        s = _make_solve(r, 8, device)
+        s.rk4(nsteps=steps)
+        s.synchronize()
+        st = torch.cuda.ExternalStream(s._lib.kg_get_stream(s.handle), device=f"cuda:{device}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.rk4(nsteps=steps)
+        e1.record(st)
+        e1.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        s.close()
+    out = {"steps": steps, "stored_points": pts, "plain_fp64_ms": plain_ms}
+    for prec in ("fp64", "mixed"):
+        b = Batch(device, precision=prec)
+        b.set_tuning(*tune)
+        solves = [_make_solve(r, 8, device) for r in reqs]
+        for s in solves:
+            b.add(s)
+        b.rk4(steps)
+        b.synchronize()
+        st = torch.cuda.ExternalStream(b.stream, device=f"cuda:{device}")
+        best = 1e30
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            b.rk4(steps)
+            e1.record(st)
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        out[f"batched_{prec}_ms"] = best
+        out[f"batched_{prec}_alg_gbs"] = pts * (1360 if prec == "fp64" else 880) * steps / (best / 1e3) / 1e9
+        for s in solves:
+            b.remove(s)
+            s.close()
+        b.close()
+    out["speedup_batched_fp64"] = plain_ms / out["batched_fp64_ms"]
+    out["speedup_batched_mixed"] = plain_ms / out["batched_mixed_ms"]
+    return out
 
 
 def _wave(d):

@@ -743,6 +743,10 @@ int launch_stage_mixed(int kind, const MixedLaunch& L, const double* rsg, int* e
 size_t mixed_item_bytes() { return sizeof(MxItem); }
 
 int build_mixed_item(void* dst, int kind, const MixedLaunch& L, const double* rsg, int* err, int kchunk, int item0) {
+  {  // equal chunks of at most the requested length (as in the FP64 batch)
+    const int nch = (L.g.NK + kchunk - 1) / kchunk;
+    kchunk = (L.g.NK + nch - 1) / nch;
+  }
   MxItem* B = reinterpret_cast<MxItem*>(dst);
   memset(B, 0, sizeof(MxItem));
   if (mx_prepare(kind, L, rsg, err, kchunk, &B->tin, &B->tp0, &B->tp1, &B->a)) return -1;

@@ -511,6 +511,13 @@ size_t batch_item_bytes() { return sizeof(BatchItem); }
 // fill one solve's item record for a batched launch of stage `kind`
 int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rsg, int* err, int kchunk,
                      int item0) {
+  // the requested chunk length is an upper bound: the solve's planes are split
+  // into equal chunks, so no chunk is a short remainder that pays a whole
+  // pipeline prologue for a few planes
+  {
+    const int nch = (L.g.NK + kchunk - 1) / kchunk;
+    kchunk = (L.g.NK + nch - 1) / nch;
+  }
   BatchItem* B = reinterpret_cast<BatchItem*>(dst);
   memset(B, 0, sizeof(BatchItem));
   if (!encode(&B->tm4, L.g, L.in[0], 4) || !encode(&B->tm1, L.g, L.in[4], 1)) return -1;
