@@ -173,6 +173,16 @@ int kg_diagnostic(kg_solver *h, int index, double *mass_out);
  * each radius is located on the vertex grid the same way (main/global_numbers.f90:152-164) */
 int kg_set_detectors(kg_solver *h, int n, const double *radii);
 /* detector radii and vertex indices (1-based) */
+/* check_point / read_from_check_point (MoL/lines_method_lib.f90:599-667), as a
+ * complete binary file: a 128-byte header (magic "KGB2CKPT", version, grid
+ * integers, metric, outer BC, scheme, precision, t, dt, ...), then u and, when
+ * the handle has them, u_stage and u_stage_2, each complex(8)
+ * u(1:5,-g:Nx+g,-g:Ny+g,0:Nz).  The stage arrays carry the previous step's Pi
+ * that PIRK stage 1 reads, so loading into a handle of the same grid resumes
+ * bit for bit (the reference's text checkpoint keeps u and t only, and its
+ * reader deletes the file before opening it). */
+int kg_save_checkpoint(kg_solver *h, const char *path);
+int kg_load_checkpoint(kg_solver *h, const char *path);
 int kg_get_detectors(kg_solver *h, double *r_det, int *index_det);
 /* proyector_detectors applied at every vertex shell r(1..Nx) (tools/FFT_sph.f90:247-279
  * at all radii): alm(l, m, shell) complex, l fastest, m = -L..L, then shell.

@@ -99,6 +99,8 @@ SIGNATURES = [
     ("kg_batch_synchronize", _I, [_P]),
     ("kg_batch_set_tuning", _I, [_P, _I, _I]),
     ("kg_batch_set_precision", _I, [_P, _I]),
+    ("kg_save_checkpoint", _I, [_P, C.c_char_p]),
+    ("kg_load_checkpoint", _I, [_P, C.c_char_p]),
     ("kg_hier_create", _I, [C.POINTER(KgParams), _I, _D, _I, _PP]),
     ("kg_hier_destroy", _I, [_P]),
     ("kg_hier_last_error", C.c_char_p, [_P]),

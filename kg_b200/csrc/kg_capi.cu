@@ -1600,6 +1600,99 @@ int kg_sph_ft_radial(kg_solver* h, int L, int Nk, int precision, double* host_ft
   return check_device_flag(h);
 }
 
+// ---- checkpoint / resume ----------------------------------------------------
+// check_point / read_from_check_point (MoL/lines_method_lib.f90:599-667) write
+// nvars, Nx, Ny, Nz, g_pts, t and, per stored point, x, y, z, u(:) as list-
+// directed text; the reader deletes the file before opening it, and neither
+// keeps the PIRK stage state that the next step reads (the previous step's Pi
+// in u_stage), so a resumed PIRK run differs from an uninterrupted one.  This
+// format is binary and complete: a 128-byte header, then u and, when they
+// exist, u_stage and u_stage_2, each as complex(8) u(1:5, -g:Nx+g, -g:Ny+g,
+// 0:Nz) (the reference's array layout, variable fastest).  Loading into a handle
+// of the same grid continues bit for bit.
+namespace {
+struct CkptHeader {
+  char magic[8];        // "KGB2CKPT"
+  int version;          // 1
+  int Nx, Ny, Nz, g_pts, metric, bc_rmax, scheme, precision;
+  int has_stage, has_stage2, reserved;
+  double t, dt, ko_eps, m, xmin, xmax;
+  char pad[128 - 8 - 12 * 4 - 6 * 8];
+};
+static_assert(sizeof(CkptHeader) == 128, "checkpoint header is 128 bytes");
+}  // namespace
+
+int kg_save_checkpoint(kg_solver* h, const char* path) {
+  if (!h || !path) return KG_EINVAL;
+  CkptHeader hd;
+  memset(&hd, 0, sizeof(hd));
+  memcpy(hd.magic, "KGB2CKPT", 8);
+  hd.version = 1;
+  hd.Nx = h->Nx; hd.Ny = h->Ny; hd.Nz = h->Nz; hd.g_pts = h->p.g_pts;
+  hd.metric = h->p.metric; hd.bc_rmax = h->p.bc_rmax; hd.scheme = h->scheme; hd.precision = h->precision;
+  hd.has_stage = h->S ? 1 : 0;
+  hd.has_stage2 = h->T ? 1 : 0;
+  hd.t = h->t; hd.dt = h->dt; hd.ko_eps = h->ko_eps; hd.m = h->p.m; hd.xmin = h->p.xmin; hd.xmax = h->p.xmax;
+  const size_t n = (size_t)5 * h->NI * h->NJ * h->NK * 2;  // doubles per state
+  std::vector<double> buf;
+  try {
+    buf.resize(n);
+  } catch (...) {
+    return set_err(h, KG_ENOMEM, "host buffer for the checkpoint");
+  }
+  FILE* f = fopen(path, "wb");
+  if (!f) return set_err(h, KG_EINVAL, std::string("cannot open for writing: ") + path);
+  int rc = KG_OK;
+  if (fwrite(&hd, sizeof(hd), 1, f) != 1) rc = set_err(h, KG_EINVAL, "checkpoint write failed");
+  const int whichs[3] = {0, 1, 2};
+  const int have[3] = {1, hd.has_stage, hd.has_stage2};
+  for (int w = 0; w < 3 && rc == KG_OK; ++w) {
+    if (!have[w]) continue;
+    if ((rc = kg_get_state(h, whichs[w], buf.data()))) break;
+    if (fwrite(buf.data(), sizeof(double), n, f) != n) rc = set_err(h, KG_EINVAL, "checkpoint write failed");
+  }
+  if (fclose(f) != 0 && rc == KG_OK) rc = set_err(h, KG_EINVAL, "checkpoint close failed");
+  return rc;
+}
+
+int kg_load_checkpoint(kg_solver* h, const char* path) {
+  if (!h || !path) return KG_EINVAL;
+  FILE* f = fopen(path, "rb");
+  if (!f) return set_err(h, KG_EINVAL, std::string("cannot open for reading: ") + path);
+  CkptHeader hd;
+  int rc = KG_OK;
+  if (fread(&hd, sizeof(hd), 1, f) != 1 || memcmp(hd.magic, "KGB2CKPT", 8) != 0 || hd.version != 1) {
+    fclose(f);
+    return set_err(h, KG_EINVAL, "not a checkpoint of this library");
+  }
+  if (hd.Nx != h->Nx || hd.Ny != h->Ny || hd.Nz != h->Nz || hd.g_pts != h->p.g_pts) {
+    fclose(f);
+    return set_err(h, KG_EINVAL, "checkpoint grid differs from the handle's grid");
+  }
+  const size_t n = (size_t)5 * h->NI * h->NJ * h->NK * 2;
+  std::vector<double> buf;
+  try {
+    buf.resize(n);
+  } catch (...) {
+    fclose(f);
+    return set_err(h, KG_ENOMEM, "host buffer for the checkpoint");
+  }
+  const int have[3] = {1, hd.has_stage, hd.has_stage2};
+  for (int w = 0; w < 3 && rc == KG_OK; ++w) {
+    if (!have[w]) continue;
+    if (fread(buf.data(), sizeof(double), n, f) != n) {
+      rc = set_err(h, KG_EINVAL, "checkpoint truncated");
+      break;
+    }
+    rc = kg_set_state(h, w, buf.data());
+  }
+  fclose(f);
+  if (rc) return rc;
+  h->t = hd.t;
+  h->dt = hd.dt;
+  return KG_OK;
+}
+
 int kg_get_detectors(kg_solver* h, double* r_det, int* index_det) {
   if (!h) return KG_EINVAL;
   for (int d = 0; d < h->n_det; ++d) {

@@ -145,6 +145,14 @@ class LinesMethod:
             raise ValueError("precision is 'fp64' or 'mixed'")
         self._ck(self._lib.kg_set_precision(self._h, 1 if mode == "mixed" else 0))
 
+    def check_point(self, path):
+        """binary checkpoint of u, the stage arrays and the clock (kg_save_checkpoint)"""
+        self._ck(self._lib.kg_save_checkpoint(self._h, str(path).encode()))
+
+    def read_from_check_point(self, path):
+        """resume from kg_save_checkpoint's file (same grid)"""
+        self._ck(self._lib.kg_load_checkpoint(self._h, str(path).encode()))
+
     def set_scheme(self, scheme, ko_eps=0.02):
         """'reference' (second order, default) or 'configured' (fourth-order
         differences, sixth-order Kreiss-Oliger dissipation of strength ko_eps,

@@ -1,0 +1,48 @@
+"""GPU tests of checkpoint/resume (kg_save_checkpoint / kg_load_checkpoint, the
+complete binary form of check_point / read_from_check_point,
+MoL/lines_method_lib.f90:599-667): a run interrupted by save + load into a new
+handle continues bit for bit, PIRK stage state included."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+G = dict(Nx=40, Ny=13, Nz=25, xmin=1.8, xmax=9.8)
+
+
+def _solver():
+    from kg_b200 import ScalarField
+    from kg_b200.initial_data import shell_ylm
+    s = ScalarField(G["Nx"], G["Ny"], G["Nz"], G["xmin"], G["xmax"], 0.25, m=0.3)
+    u0, _ = shell_ylm(G["Nx"], G["Ny"], G["Nz"], G["xmin"], G["xmax"], seed=4, r0=5.0, sd=1.0)
+    s.u = u0
+    return s
+
+
+@pytest.mark.parametrize("method", ["pirk2", "pirk3", "rk4"])
+def test_resume_is_bitexact(tmp_path, method):
+    from kg_b200 import ScalarField
+    step = (lambda s, n: getattr(s, method)(nsteps=n)) if method.startswith("rk") else \
+        (lambda s, n: getattr(s, method)(n))
+    a = _solver()
+    step(a, 3)
+    path = tmp_path / "ckpt.bin"
+    a.check_point(path)
+    step(a, 4)
+    b = ScalarField(G["Nx"], G["Ny"], G["Nz"], G["xmin"], G["xmax"], 0.25, m=0.3)
+    b.read_from_check_point(path)
+    step(b, 4)
+    assert np.array_equal(a.u, b.u)
+    assert a.t == b.t
+
+
+def test_checkpoint_grid_mismatch_is_rejected(tmp_path):
+    from kg_b200 import ScalarField, KgError
+    a = _solver()
+    path = tmp_path / "ckpt.bin"
+    a.check_point(path)
+    c = ScalarField(G["Nx"] + 8, G["Ny"], G["Nz"], G["xmin"], G["xmax"], 0.25, m=0.3)
+    with pytest.raises(KgError):
+        c.read_from_check_point(path)
+    with pytest.raises(KgError):
+        c.read_from_check_point(tmp_path / "missing.bin")
