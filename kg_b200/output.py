@@ -94,3 +94,69 @@ def read_lm(path):
             arr = np.array([[float(x) for x in r] for r in rows])
             blocks.append((arr[:, 0].astype(int), arr[:, 1].astype(int), arr[:, 2] + 1j * arr[:, 3]))
     return blocks
+
+
+class AsyncSnapshots:
+    """3-D snapshots of the state while the solve keeps stepping: the reference
+    writes HDF5 files of the fields every save_3d steps (hdf5/hdf5_lib.f90, from
+    save_gnuplot); here `snap(index)` copies u on the device (kg_get_state_device,
+    ordered on the solver's stream) into one of `depth` device buffers and a
+    worker thread moves it to pinned host memory and writes
+    `<prefix>_<index>.npy` (complex128, shape (Nz+1, Ny+2g+1, Nx+2g+1, 5), the
+    reference's u(1:5,-g:Nx+g,-g:Ny+g,0:Nz) memory order) with the time in
+    `<prefix>_<index>.t`.  The solver's stream only waits for the device copy."""
+
+    def __init__(self, solver, directory=".", prefix="u", depth=2):
+        import queue
+        import threading
+        import torch
+        import ctypes as C
+        self.s, self.dir, self.prefix = solver, directory, prefix
+        os.makedirs(directory, exist_ok=True)
+        dev = f"cuda:{max(torch.cuda.current_device(), 0)}"
+        shape = (solver.NK, solver.NJ, solver.NI, 5)
+        self._bufs = [torch.empty(shape, dtype=torch.complex128, device=dev) for _ in range(depth)]
+        self._free = queue.Queue()
+        for i in range(depth):
+            self._free.put(i)
+        self._work = queue.Queue()
+        self._host = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+        self._C = C
+        self._err = None
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+
+    def snap(self, index):
+        import torch
+        i = self._free.get()                       # waits only if `depth` snapshots are in flight
+        s = self.s
+        s._ck(s._lib.kg_get_state_device(s.handle, 0, self._C.c_void_p(self._bufs[i].data_ptr())))
+        stream = torch.cuda.ExternalStream(s._lib.kg_get_stream(s.handle))
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        self._work.put((i, ev, int(index), s.t))
+
+    def _run(self):
+        while True:
+            item = self._work.get()
+            if item is None:
+                return
+            i, ev, index, t = item
+            try:
+                ev.synchronize()
+                self._host.copy_(self._bufs[i])
+                base = os.path.join(self.dir, f"{self.prefix}_{index:08d}")
+                np.save(base + ".npy", self._host.numpy())
+                with open(base + ".t", "w") as f:
+                    f.write(f"{float(t)!r}\n")
+            except Exception as e:  # reported by close()
+                self._err = e
+            finally:
+                self._free.put(i)
+
+    def close(self):
+        """wait for every snapshot to be on disk"""
+        self._work.put(None)
+        self._thread.join()
+        if self._err is not None:
+            raise self._err

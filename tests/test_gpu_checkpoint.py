@@ -46,3 +46,20 @@ def test_checkpoint_grid_mismatch_is_rejected(tmp_path):
         c.read_from_check_point(path)
     with pytest.raises(KgError):
         c.read_from_check_point(tmp_path / "missing.bin")
+
+
+def test_async_snapshots_match_the_state_at_their_step(tmp_path):
+    from kg_b200.output import AsyncSnapshots
+    a = _solver()
+    snaps = AsyncSnapshots(a, str(tmp_path), depth=2)
+    want = {}
+    for i in range(1, 7):
+        a.pirk2(1)
+        if i % 2 == 0:
+            snaps.snap(i)
+            want[i] = (a.u.copy(), a.t)
+    snaps.close()
+    for i, (u, t) in want.items():
+        got = np.load(tmp_path / f"u_{i:08d}.npy")
+        assert np.array_equal(got, u)
+        assert float(open(tmp_path / f"u_{i:08d}.t").read()) == t
