@@ -477,7 +477,8 @@ def projection_leg(mol, lib, h, L=64, reps=3):
 
 
 def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
+    from kg_b200 import replicas
+    _, rank, _ = replicas.rank_env()
     if rank != 0:
         return 0
     w = WORKLOAD
@@ -537,32 +538,26 @@ def main():
         return run_reference(args)
 
     import torch
-    import torch.distributed as dist
-    from kg_b200 import ScalarField
+    from kg_b200 import ScalarField, replicas
     from kg_b200.initial_data import shell_ylm_device
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = replicas.rank_env()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    replicas.init(world, backend="nccl", timeout_s=120)
     w = WORKLOAD
     mol = ScalarField(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], m=w["m"], device=local,
                       save=10 * 0.25 * 0.0018, l_max=8)
     lib, h = mol._lib, mol.handle
     if args.variant is not None:
         mol._ck(lib.kg_set_kernel_variant(h, args.variant))
-    u0, _ = shell_ylm_device(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], seed=w["seed"] + rank,
-                             device=f"cuda:{local}")
+    u0, _ = shell_ylm_device(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"],
+                             seed=replicas.replica_seed(w["seed"], rank), device=f"cuda:{local}")
     mol._ck(lib.kg_set_state_device(h, 0, C.c_void_p(u0.data_ptr())))
     mol.synchronize()
     stream = torch.cuda.ExternalStream(lib.kg_get_stream(h), device=f"cuda:{local}")
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        replicas.barrier(world)
 
     # ---- device-resident timing
     for _ in range(args.warmup):
@@ -589,10 +584,7 @@ def main():
     el_ms = e0.elapsed_time(e1)
     lib.kg_profile_read(h, ms, cnt)
     lib.kg_profile_enable(h, 0)
-    t = torch.tensor([el_ms], device=f"cuda:{local}", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    el_ms = float(t.item())
+    el_ms = replicas.max_over_ranks(el_ms, world, device=f"cuda:{local}")
     kinds = {lib.kg_profile_kind_name(i).decode(): (ms[i], cnt[i]) for i in range(nk) if cnt[i] > 0}
 
     # other steppers, briefly (device-resident, same grid)
@@ -632,14 +624,11 @@ def main():
         mol._ck(lib.kg_get_state(h, 0, p_out))
     f1.record(stream)
     f1.synchronize()
-    t = torch.tensor([f0.elapsed_time(f1)], device=f"cuda:{local}", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t.item())
+    e2e_ms = replicas.max_over_ranks(f0.elapsed_time(f1), world, device=f"cuda:{local}")
 
     pts = interior_points(w)
-    value = world * pts * 2 * args.steps / (el_ms / 1e3)
-    e2e_value = world * pts * 2 * args.steps / (e2e_ms / 1e3)
+    value = replicas.job_rate(pts * 2 * args.steps, world, el_ms)
+    e2e_value = replicas.job_rate(pts * 2 * args.steps, world, e2e_ms)
 
     # roofline of the dominant kernel
     stage_kinds = {k: v for k, v in kinds.items() if k in ALG_BYTES}
@@ -687,9 +676,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     mol.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(world)
     return 0
 
 
