@@ -242,6 +242,13 @@ int kg_batch_synchronize(kg_batch *b);
 int kg_batch_set_tuning(kg_batch *b, int kchunk, int blocks);
 /* 0 = FP64 RK4 for every member (default), 1 = mixed precision as kg_set_precision */
 int kg_batch_set_precision(kg_batch *b, int mode);
+/* proyector_detectors (MoL/diagnostic_lib.f90:231-250) for every member at once,
+ * ordered behind the batch's steps, one synchronisation: host_alm receives each
+ * member's a_lm(0:L, -L:L, n_det) block (as kg_proyector_detectors writes it) in
+ * member order. */
+int kg_batch_proyector_detectors(kg_batch *b, double *host_alm);
+/* complex values kg_batch_proyector_detectors writes (sum over members) */
+long long kg_batch_alm_count(const kg_batch *b);
 int kg_batch_get_tuning(const kg_batch *b, int *kchunk, int *blocks);
 long long kg_batch_launch_count(const kg_batch *b);
 void *kg_batch_get_stream(const kg_batch *b);

@@ -72,6 +72,22 @@ class Batch:
     def synchronize(self):
         self._ck(self._lib.kg_batch_synchronize(self._b))
 
+    def proyector_detectors(self):
+        """every member's detector a_lm (n_det, 2L+1, L+1), in member order, from
+        one batched launch sequence and one synchronisation"""
+        sizes = [(m.n_det, 2 * m.l_max + 1, m.l_max + 1) for m in self.members]
+        out = np.zeros(sum(a * b * c for a, b, c in sizes), np.complex128)
+        if self._lib.kg_batch_alm_count(self._b) != out.size:
+            raise RuntimeError("batch members' detector tables differ from their Python views")
+        if out.size:
+            self._ck(self._lib.kg_batch_proyector_detectors(
+                self._b, out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))))
+        res, off = [], 0
+        for a, b, c in sizes:
+            res.append(out[off:off + a * b * c].reshape(a, b, c))
+            off += a * b * c
+        return res
+
     def set_tuning(self, kchunk, blocks):
         self._ck(self._lib.kg_batch_set_tuning(self._b, int(kchunk), int(blocks)))
 

@@ -99,6 +99,8 @@ SIGNATURES = [
     ("kg_batch_synchronize", _I, [_P]),
     ("kg_batch_set_tuning", _I, [_P, _I, _I]),
     ("kg_batch_set_precision", _I, [_P, _I]),
+    ("kg_batch_proyector_detectors", _I, [_P, _D]),
+    ("kg_batch_alm_count", C.c_longlong, [_P]),
     ("kg_save_checkpoint", _I, [_P, C.c_char_p]),
     ("kg_load_checkpoint", _I, [_P, C.c_char_p]),
     ("kg_hier_create", _I, [C.POINTER(KgParams), _I, _D, _I, _PP]),

@@ -1791,6 +1791,8 @@ struct kg_batch {
   long long graph_launches = 0;
   long long launches = 0;
   cudaEvent_t ev = nullptr;
+  double2* pin = nullptr;  // pinned staging of the members' detector a_lm
+  size_t pin_cap = 0;
 };
 
 #define KG_BCK(call)                                                        \
@@ -1975,6 +1977,7 @@ int kg_batch_destroy(kg_batch* b) {
   }
   for (int st = 0; st < 3; ++st)
     if (b->dghost_f[st]) cudaFree(b->dghost_f[st]);
+  if (b->pin) cudaFreeHost(b->pin);
   if (b->derr) cudaFree(b->derr);
   if (b->ev) cudaEventDestroy(b->ev);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -2068,6 +2071,58 @@ int kg_batch_rk4(kg_batch* b, int nsteps) {
   // members' later work waits for the batch
   KG_BCK(cudaEventRecord(b->ev, b->stream));
   for (kg_solver* h : b->members) KG_BCK(cudaStreamWaitEvent(h->stream, b->ev, 0));
+  return KG_OK;
+}
+
+// proyector_detectors (MoL/diagnostic_lib.f90:231-250) of every member, enqueued
+// on the batch stream behind its steps, with one synchronisation for all of
+// them: host_alm receives the members' a_lm(n_det, -L:L, 0:L) blocks in member
+// order (zeros for detectors outside the grid).
+long long kg_batch_alm_count(const kg_batch* b) {
+  if (!b) return -1;
+  long long total = 0;
+  for (kg_solver* h : b->members) total += (long long)(h->L + 1) * (2 * h->L + 1) * h->n_det;
+  return total;
+}
+
+int kg_batch_proyector_detectors(kg_batch* b, double* host_alm) {
+  if (!b || !host_alm) return KG_EINVAL;
+  size_t total = 0;
+  for (kg_solver* h : b->members) total += (size_t)(h->L + 1) * (2 * h->L + 1) * h->n_det;
+  if (total == 0) return KG_OK;
+  if (total > b->pin_cap) {
+    if (b->pin) cudaFreeHost(b->pin);
+    b->pin = nullptr;
+    b->pin_cap = 0;
+    KG_BCK(cudaMallocHost((void**)&b->pin, 2 * total * sizeof(double2)));
+    b->pin_cap = 2 * total;
+  }
+  for (kg_solver* h : b->members) {
+    KG_BCK(cudaEventRecord(b->ev, h->stream));
+    KG_BCK(cudaStreamWaitEvent(b->stream, b->ev, 0));
+  }
+  size_t off = 0;
+  for (kg_solver* h : b->members) {
+    const size_t n = (size_t)(h->L + 1) * (2 * h->L + 1) * h->n_det;
+    kg::launch_shell_interp(h->g, metric_of(h), h->U, h->si, h->n_det, h->Ny, h->Nz, 1, h->shells, b->stream);
+    kg::launch_project(h->shells, h->si.active, h->n_det, h->L, h->Ny, h->Nz, h->normP, h->cosm, h->sinm, h->sint,
+                       h->dy * h->dz, h->alm, b->stream);
+    KG_BCK(cudaMemcpyAsync(b->pin + off, h->alm, n * sizeof(double2), cudaMemcpyDeviceToHost, b->stream));
+    off += n;
+  }
+  b->launches += 2 * (long long)b->members.size();
+  KG_BCK(cudaGetLastError());
+  KG_BCK(cudaStreamSynchronize(b->stream));
+  off = 0;
+  for (kg_solver* h : b->members) {
+    const size_t per = (size_t)(h->L + 1) * (2 * h->L + 1);
+    for (int d = 0; d < h->n_det; ++d) {
+      double2* dst = reinterpret_cast<double2*>(host_alm) + off + per * d;
+      if (h->active[d]) memcpy(dst, b->pin + off + per * d, per * sizeof(double2));
+      else memset(dst, 0, per * sizeof(double2));
+    }
+    off += per * h->n_det;
+  }
   return KG_OK;
 }
 

@@ -185,11 +185,13 @@ class Server:
                 continue
             peak_live = max(peak_live, len(live))
             batch.rk4(self.q)
+            # every live solve's waveform sample from one batched launch sequence
+            samples = batch.proyector_detectors()
             still = []
-            for entry in live:
+            for entry, a in zip(live, samples):
                 r, s = entry[0], entry[1]
                 entry[2] += self.q
-                entry[5].append(self._sample(s))
+                entry[5].append(a[0].copy())
                 entry[4].append(s.t)
                 if entry[2] >= r.steps:
                     done = time.perf_counter() - t0
