@@ -96,6 +96,12 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
   const int ii0 = bx * TI, jj0 = by * TJ;
   const int ii = ii0 + tx, jj = jj0 + ty;
   const bool act = (ii < g.NI) && (jj < g.NJ);
+  // ring slot protocol: full[s] (bars[s]) completes when a plane's boxes have
+  // landed; empty[s] when all eight warps have read the plane for the last
+  // time, after which thread 0 may load the next plane into the slot, so the
+  // warps are not held at a block barrier per plane
+  uint64_t* empty = bars + NST;
+  const int lane = tid & 31;
   const int k0 = bz * a.kchunk;
   if (k0 >= g.NK) return 0;
   const int k1 = min(k0 + a.kchunk, g.NK);
@@ -107,6 +113,10 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
   };
   auto slot = [&](int t) -> int { return (int)((tb + (uint32_t)t) % NST); };
   auto parity = [&](int t) -> uint32_t { return ((tb + (uint32_t)t) / NST) & 1u; };
+  auto release = [&](int t) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[slot(t)]);
+  };
   auto issue = [&](int t) {
     const int s = slot(t);
     uint64_t* b = &bars[s];
@@ -186,22 +196,31 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
     if (PSI) Epv = phiE(st);
     if (PI_) Fpv = phiF(st);
   }
+  release(0);
   bool failed = __syncthreads_or(timed_out) != 0;
+  const int last = k1 - k0 - 1;
 
-  for (int i = 0; i < k1 - k0 && !failed; ++i) {
+  for (int i = 0; i <= last && !failed; ++i) {
     const int k = k0 + i;
-    if (tid == 0) {
+    if (tid == 0 && !timed_out) {
       if (i + NST < nplanes) {
-        issue(i + NST);
-        nissued = i + NST + 1;
+        // plane i shares the slot; every warp released it after its last use
+        if (mbar_wait_bounded(&empty[slot(i)], parity(i))) {
+          issue(i + NST);
+          nissued = i + NST + 1;
+        } else {
+          timed_out = 1;
+        }
       }
       prefetch(k + 2);
     }
     {
       const int tc = i + 1, tn = i + 2;
-      const bool okc = mbar_wait_bounded(&bars[slot(tc)], parity(tc));
-      const bool okn = okc && mbar_wait_bounded(&bars[slot(tn)], parity(tn));
-      if (!okn) timed_out = 1;
+      if (!timed_out) {
+        const bool okc = mbar_wait_bounded(&bars[slot(tc)], parity(tc));
+        const bool okn = okc && mbar_wait_bounded(&bars[slot(tn)], parity(tn));
+        if (!okn) timed_out = 1;
+      }
       if (act && !timed_out) {
         const double* cu = ring + (size_t)slot(tc) * STAGE_D;
         const double* nx = ring + (size_t)slot(tn) * STAGE_D;
@@ -352,8 +371,10 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
         Fcu = Fnx;
       }
     }
-    failed = __syncthreads_or(timed_out) != 0;
+    release(i + 1);
+    if (i == last) release(i + 2);
   }
+  failed = __syncthreads_or(timed_out) != 0;
   if (failed) {
     if (tid == 0) {
       atomicExch(a.err, 1);
@@ -381,6 +402,7 @@ __device__ __forceinline__ unsigned char* align128(unsigned char* p) {
 __device__ __forceinline__ void init_ring_barriers(uint64_t* bars) {
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[NST + s], TI * TJ / 32);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();

@@ -2,7 +2,7 @@
 
 The FP64 solver keeps the reference's operation order and rounding (no fused
 multiply-add, component-wise complex-by-real arithmetic), so states after any
-number of steps are compared for exact equality.  The north-star bound for
+number of steps are compared for exact equality.  The parity bound for
 the C0 run is 1e-11 relative L2 in phi and Pi after 1000 steps; the test
 asserts that bound and, separately, reports bit equality.
 Diagnostics that reduce in a different order are compared at 1e-12 relative.
