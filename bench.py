@@ -164,6 +164,44 @@ SERVE_DESC = ("scaled serving workload: Poisson arrivals at 2000/s (the offered 
               "one GPU's HBM roofline, so it is scaled down in count, grid and steps")
 
 
+BATCH_DESC = ("batching form: 512 solves drawn from seed 20240603 (Nr ~ U{128..1024 step 64} on r in "
+              "[1.8, 1.8+0.1 Nr], Ntheta in {16, 32, 64}, Nphi = 2 Ntheta, m ~ U[0, 0.5], shell r0 ~ U[6, 15], "
+              "sigma ~ U[0.8, 2], c_lm (l<=4) N(0, 1e-4)), RK4; all 512 in FP64 exceed HBM, so they run in "
+              "admission waves: the first wave (draw order, 120 GB FP64 budget) is timed over a few steps, plain "
+              "FP64 one solve at a time against the same solves batched in FP64 and in the mixed form")
+
+
+def batch_leg(device, steps=5, budget=120e9, count=512):
+    """The batching form on its own solve mix: device time of `steps` RK4 steps of
+    the first admission wave, plain FP64 (one solve after another) against one
+    persistent launch per stage over all of them (FP64 and mixed)."""
+    import torch
+    from kg_b200.serve import draw_requests, _bytes_estimate
+    from kg_b200.batch import autotune
+    reqs = draw_requests(seed=20240603, rate=100.0, count=count, nr=(128, 1024), nr_step=64,
+                         ntheta=(16, 32, 64), steps=(2000, 2000), quantum=10)
+    waves, cur, used = [], [], 0.0
+    for r in reqs:
+        b = _bytes_estimate(r, "fp64")
+        if cur and used + b > budget:
+            waves.append(cur)
+            cur, used = [], 0.0
+        cur.append(r)
+        used += b
+    waves.append(cur)
+    wave = waves[0]
+    shapes = sorted({(r.grid()["Nx"], r.grid()["Ny"], r.grid()["Nz"]) for r in wave})
+    tune = autotune(shapes[:: max(1, len(shapes) // 6)], device=device, kchunks=(16, 32, 64), steps=2)
+    torch.cuda.empty_cache()
+    eng = engine_leg(wave, device, tune, steps=steps)
+    interior = sum(r.Nr * r.Ntheta * 2 * r.Ntheta for r in wave)
+    gpsu = lambda ms: interior * 4 * steps / (ms / 1e3)
+    return {"workload": BATCH_DESC, "solves_drawn": count, "waves_for_all": len(waves), "wave_solves": len(wave),
+            "wave_interior_points": interior, "tuning": list(tune), "engine_device_time": eng,
+            "gpsu": {"plain_fp64": gpsu(eng["plain_fp64_ms"]), "batched_fp64": gpsu(eng["batched_fp64_ms"]),
+                     "batched_mixed": gpsu(eng["batched_mixed_ms"])}}
+
+
 def serve_leg(count, device):
     """plain FP64 (one solve at a time) vs continuous batching, FP64 and mixed, on the same requests"""
     from kg_b200.serve import Server, draw_requests, waveform_error_detail
@@ -527,6 +565,7 @@ def main():
     ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-refinement", action="store_true", help="skip the Berger-Oliger leg")
     ap.add_argument("--no-c0", action="store_true", help="skip the configured-method test-field leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batching-form leg")
     args = ap.parse_args()
     if args.grid:
         nx, ny, nz = (int(v) for v in args.grid.split(","))
@@ -657,7 +696,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_projection:
         line["projection"] = projection_leg(mol, lib, h)
     if rank == 0 and world == 1 and not args.grid and not (args.no_precision and args.no_serve and
-                                                            args.no_refinement and args.no_c0):
+                                                            args.no_refinement and args.no_c0 and args.no_batch):
         mol.close()  # the legs below allocate their own solves
         torch.cuda.empty_cache()
         if not args.no_precision:
@@ -666,6 +705,8 @@ def main():
             line["refinement"] = refinement_leg(w, local)
         if not args.no_c0:
             line["c0_configured"] = c0_leg(local)
+        if not args.no_batch:
+            line["batching"] = batch_leg(local)
         if not args.no_serve:
             line["serving"] = serve_leg(args.serve_count, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -2,7 +2,7 @@
 
     python -m kg_b200.profile_cases mixed      [--grid Nx,Ny,Nz] [--steps K]
     python -m kg_b200.profile_cases configured [--grid Nx,Ny,Nz] [--steps K]
-    python -m kg_b200.profile_cases batch      [--solves N] [--precision fp64|mixed] [--steps K]
+    python -m kg_b200.profile_cases batch      [--solves N] [--precision fp64|mixed] [--mix serving|c3] [--steps K]
     python -m kg_b200.profile_cases refine     [--grid Nx,Ny,Nz] [--steps K]
 
 Each case builds seeded synthetic input on the device, runs K steps and exits
@@ -10,8 +10,10 @@ Each case builds seeded synthetic input on the device, runs K steps and exits
 L2, so a profiler capture of one launch is representative and ends quickly.
   mixed:      RK4 with the FP32 stencil RHS and FP64 update (mixed_rk4_* kernels)
   configured: RK4 of the fourth-order method (cfg_stage_kernel)
-  batch:      the serving request mix advanced as one batch (tma_batch_kernel /
-              mx_batch_kernel, persistent over a ragged work list)
+  batch:      a request mix advanced as one batch (tma_batch_kernel /
+              mx_batch_kernel, persistent over a ragged work list): the serving
+              mix (Nr 128..512, Ntheta 16/32) or the batching-form mix
+              (Nr 128..1024, Ntheta 16/32/64)
   refine:     a two-level Berger-Oliger hierarchy (prolong/restrict kernels)
 """
 from __future__ import annotations
@@ -39,6 +41,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--solves", type=int, default=30)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--mix", default="serving", choices=["serving", "c3"])
+    ap.add_argument("--kchunk", type=int, default=64)
     a = ap.parse_args(argv)
     from .lines_method import ScalarField
     if a.case == "mixed":
@@ -63,10 +67,14 @@ def main(argv=None):
     elif a.case == "batch":
         from .batch import Batch
         from .serve import draw_requests, _make_solve
-        reqs = draw_requests(seed=20240602, rate=2000.0, count=a.solves, nr=(128, 512), nr_step=64,
-                             ntheta=(16, 32), steps=(100, 1000), quantum=10)
+        if a.mix == "serving":
+            reqs = draw_requests(seed=20240602, rate=2000.0, count=a.solves, nr=(128, 512), nr_step=64,
+                                 ntheta=(16, 32), steps=(100, 1000), quantum=10)
+        else:
+            reqs = draw_requests(seed=20240603, rate=100.0, count=a.solves, nr=(128, 1024), nr_step=64,
+                                 ntheta=(16, 32, 64), steps=(2000, 2000), quantum=10)
         b = Batch(0, precision=a.precision)
-        b.set_tuning(64, 296)
+        b.set_tuning(a.kchunk, 296)
         solves = [_make_solve(r, 8, 0) for r in reqs]
         for s in solves:
             b.add(s)
