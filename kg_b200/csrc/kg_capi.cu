@@ -14,6 +14,8 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -123,16 +125,74 @@ int set_err(kg_solver* h, int code, const std::string& msg) {
   return code;
 }
 
+// Solver buffers come from one stream-ordered memory pool per device: a
+// serving loop creates and destroys solves continuously, and cudaMalloc /
+// cudaFree would synchronise the whole device at every creation and
+// retirement; pool allocations and frees are ordered on the solver's stream
+// and freed blocks are reused.  Up to POOL_KEEP bytes of freed blocks stay
+// reserved for reuse; an allocation that finds the device full gives every
+// cached block back and retries once.
+constexpr uint64_t POOL_KEEP = 32ull << 30;
+constexpr int POOL_DEVICES = 64;
+
+cudaMemPool_t solver_pool(int dev) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[POOL_DEVICES] = {};
+  if (dev < 0 || dev >= POOL_DEVICES) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps pr;
+    memset(&pr, 0, sizeof(pr));
+    pr.allocType = cudaMemAllocationTypePinned;
+    pr.handleTypes = cudaMemHandleTypeNone;
+    pr.location.type = cudaMemLocationTypeDevice;
+    pr.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &pr) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t keep = POOL_KEEP;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = pool;
+  }
+  return pools[dev];
+}
+
 int dalloc(kg_solver* h, void** p, size_t n) {
-  cudaError_t e = cudaMalloc(p, n);
+  *p = nullptr;
+  cudaMemPool_t pool = solver_pool(h->device);
+  if (!pool) {
+    h->err = "no device memory pool";
+    return KG_ECUDA;
+  }
+  cudaError_t e = cudaMallocFromPoolAsync(p, n, pool, h->stream);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    cudaDeviceSynchronize();  // pending frees complete, then the cache is released
+    cudaMemPoolTrimTo(pool, 0);
+    e = cudaMallocFromPoolAsync(p, n, pool, h->stream);
+  }
   if (e != cudaSuccess) {
-    h->err = std::string("cudaMalloc(") + std::to_string(n) + "): " + cudaGetErrorString(e);
+    cudaGetLastError();
+    h->err = std::string("device allocation of ") + std::to_string(n) + " bytes: " + cudaGetErrorString(e);
     *p = nullptr;
     return KG_ENOMEM;
+  }
+  if (reinterpret_cast<uintptr_t>(*p) & 255u) {  // rows and TMA boxes assume 256-byte aligned bases
+    cudaFreeAsync(*p, h->stream);
+    *p = nullptr;
+    h->err = "device allocation not 256-byte aligned";
+    return KG_ECUDA;
   }
   h->bytes += n;
   cudaMemsetAsync(*p, 0, n, h->stream);
   return KG_OK;
+}
+
+// returns a dalloc block to the pool, ordered after the solver's queued work
+void dfree(kg_solver* h, void* p) {
+  if (p) cudaFreeAsync(p, h->stream);
 }
 
 size_t field_bytes(const kg_solver* h) { return (size_t)h->g.fs * sizeof(double2); }
@@ -439,7 +499,7 @@ int build_detectors(kg_solver* h, const double* radii = nullptr) {
   }
   for (void** p : {(void**)&h->d_int, (void**)&h->d_dbl, (void**)&h->shells, (void**)&h->alm, (void**)&h->flux})
     if (*p) {
-      cudaFree(*p);
+      dfree(h, *p);
       *p = nullptr;
     }
   auto rv = [&](int iv) { return h->xmin + (double)(iv - 1) * h->dx; };
@@ -712,8 +772,9 @@ int kg_create(const kg_params* p, int device, kg_solver** out) {
   }
   int dev = 0;
   cudaGetDevice(&dev);
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || prop.major < 10) return KG_ENODEV;
+  int major = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess || major < 10)
+    return KG_ENODEV;
   kg_solver* h = new kg_solver();
   h->p = *p;
   h->device = dev;
@@ -758,8 +819,7 @@ int kg_destroy(kg_solver* h) {
   void* bufs[] = {h->dmet, h->U, h->S, h->T, h->RK, h->UP, h->HV, h->stage_buf, h->rho, h->partials,
                   h->d_int, h->d_dbl, h->shells, h->alm, h->flux, h->derr, h->ylm_tab, h->ylm_buf,
                   h->rad_jr, h->rad_ft, h->MX, h->mx_gdesc};
-  for (void* b : bufs)
-    if (b) cudaFree(b);
+  for (void* b : bufs) dfree(h, b);
   for (auto& row : h->graphs)
     for (auto& e : row)
       if (e.exec) cudaGraphExecDestroy(e.exec);
@@ -1448,7 +1508,7 @@ int project_all(kg_solver* h, int L, int precision, double2** out_alm) {
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t need = 2 * al(szA) + 2 * al(szB) + al(szC) + al(szF) + al(szAlm);
   if (h->ylmL != L) {
-    if (h->ylm_tab) cudaFree(h->ylm_tab);
+    dfree(h, h->ylm_tab);
     h->ylm_tab = nullptr;
     std::vector<double> tab((size_t)(L + 1) * (L + 1) * Ny + 2 * (size_t)(L + 1) * Nz, 0.0);
     double* normP = tab.data();
@@ -1471,7 +1531,7 @@ int project_all(kg_solver* h, int L, int precision, double2** out_alm) {
     h->ylm_b_ready = 0;
   }
   if (h->ylm_bytes < need) {
-    if (h->ylm_buf) cudaFree(h->ylm_buf);
+    dfree(h, h->ylm_buf);
     h->ylm_buf = nullptr;
     int rc = dalloc(h, (void**)&h->ylm_buf, need);
     if (rc) return rc;
@@ -1539,7 +1599,7 @@ int ensure_radial_basis(kg_solver* h, int L, int Nk) {
       }
   for (void** p : {(void**)&h->rad_jr, (void**)&h->rad_ft})
     if (*p) {
-      cudaFree(*p);
+      dfree(h, *p);
       *p = nullptr;
     }
   int rc;
@@ -2280,6 +2340,12 @@ int kg_hier_create(const kg_params* base, int nlevels, const double* r_fine, int
     }
     H->uold.push_back(b);
   }
+  for (kg_solver* h : H->lv)  // the level copies exist before any level's stream uses them
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+      H->err = "allocating level copies failed";
+      kg_hier_destroy(H);
+      return KG_ECUDA;
+    }
   H->ev.resize(nlevels);
   for (auto& e : H->ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   *out = H;
@@ -2290,8 +2356,7 @@ int kg_hier_destroy(kg_hier* H) {
   if (!H) return KG_EINVAL;
   for (kg_solver* h : H->lv)
     if (h) cudaStreamSynchronize(h->stream);
-  for (double2* b : H->uold)
-    if (b) cudaFree(b);
+  for (size_t l = 0; l < H->uold.size(); ++l) dfree(H->lv[l], H->uold[l]);
   for (auto e : H->ev)
     if (e) cudaEventDestroy(e);
   for (kg_solver* h : H->lv)

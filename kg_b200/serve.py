@@ -6,9 +6,9 @@ live solve's state on the device, advances all live solves together through
 the batched engine (one persistent launch per RK4 stage over all of them, a
 step replayed from a CUDA graph), samples each solve's l <= l_max waveform
 a_lm(t) at r_ext = 0.8 r_max every `save_every` steps, and retires a solve --
-returning its waveform -- as soon as it has run its steps.  New arrivals join
-between batch quanta, so requests that arrive while others are on the GPU
-overlap with them.
+returning its waveform -- as soon as it has run its steps.  New arrivals are
+set up (host and device) while a quantum runs and step from the next one, so
+requests that arrive while others are on the GPU overlap with them.
 
 `mode="plain"` serves the same requests one at a time through the single-solve
 path (kg_rk4 on its own handle), the baseline the batched form is compared
@@ -169,40 +169,46 @@ class Server:
             while i_next < len(reqs) and reqs[i_next].arrival <= now:
                 pending.append(reqs[i_next])
                 i_next += 1
-            # admission against the HBM budget, first come first served
-            while pending and len(live) < self.max_live and \
+            stepping = bool(live)
+            if stepping:
+                peak_live = max(peak_live, len(live))
+                batch.rk4(self.q)  # queued on the device; the host prepares arrivals meanwhile
+            # admission against the HBM budget, first come first served: the new
+            # solves are created and join the batch while the quantum runs; they
+            # are appended after the live members, and step from the next quantum
+            joined = []
+            while pending and len(live) + len(joined) < self.max_live and \
                     used + _bytes_estimate(pending[0], self.precision) <= self.budget:
                 r = pending.popleft()
                 s = _make_solve(r, self.l_max, self.device)
                 batch.add(s)
                 used += _bytes_estimate(r, self.precision)
-                live.append([r, s, 0, time.perf_counter() - t0, [], []])
+                joined.append([r, s, 0, time.perf_counter() - t0, [], []])
+            still = []
+            if stepping:
+                # every member's waveform sample from one batched launch sequence;
+                # the live solves are the first len(live) members
+                samples = batch.proyector_detectors()
+                for entry, a in zip(live, samples):
+                    r, s = entry[0], entry[1]
+                    entry[2] += self.q
+                    entry[5].append(a[0].copy())
+                    entry[4].append(s.t)
+                    if entry[2] >= r.steps:
+                        done = time.perf_counter() - t0
+                        batch.remove(s)
+                        results.append(Result(r.rid, r.arrival, entry[3], done, r.steps, np.array(entry[4]),
+                                              np.array(entry[5])))
+                        used -= _bytes_estimate(r, self.precision)
+                        s.close()
+                    else:
+                        still.append(entry)
+            live = still + joined
             if not live:
                 if pending:
                     raise RuntimeError("a single request exceeds the HBM budget")
                 if i_next < len(reqs):
                     time.sleep(max(0.0, reqs[i_next].arrival - (time.perf_counter() - t0)))
-                continue
-            peak_live = max(peak_live, len(live))
-            batch.rk4(self.q)
-            # every live solve's waveform sample from one batched launch sequence
-            samples = batch.proyector_detectors()
-            still = []
-            for entry, a in zip(live, samples):
-                r, s = entry[0], entry[1]
-                entry[2] += self.q
-                entry[5].append(a[0].copy())
-                entry[4].append(s.t)
-                if entry[2] >= r.steps:
-                    done = time.perf_counter() - t0
-                    batch.remove(s)
-                    results.append(Result(r.rid, r.arrival, entry[3], done, r.steps, np.array(entry[4]),
-                                          np.array(entry[5])))
-                    used -= _bytes_estimate(r, self.precision)
-                    s.close()
-                else:
-                    still.append(entry)
-            live = still
         wall = time.perf_counter() - t0
         batch.close()
         out = self._summary(results, wall)
