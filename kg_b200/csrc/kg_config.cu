@@ -25,8 +25,10 @@
 #include <cuda_runtime.h>
 #include "kg_device.cuh"
 #include "kg_internal.h"
+#include "kg_tma_ops.cuh"
 
 namespace kg {
+using namespace tmaops;
 namespace {
 
 struct CfgArgs {
@@ -82,18 +84,16 @@ __device__ __forceinline__ double2 ko6(double2 m3, double2 m2, double2 m1, doubl
 }
 __device__ __forceinline__ double2 cdiv(double2 a, double s) { return c2(a.x / s, a.y / s); }
 
-template <int KIND>
-__global__ void __launch_bounds__(128) cfg_stage_kernel(CfgArgs a) {
+// RHS and RK4 combination at one stored point (ii, jj, k).  S(v, i, j) returns
+// variable v of the stage input at (i, j) on plane k, P(v, kk) at the point's
+// own (ii, jj) on plane kk; the two kernels below differ only in where S and P
+// read from, so they produce the same bits.
+template <int KIND, class SF, class PF>
+__device__ __forceinline__ void cfg_point(const CfgArgs& a, int ii, int jj, int k, const SF& S, const PF& P) {
   const Grid& g = a.g;
   const Metric& M = a.m;
-  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
-  const int jj = blockIdx.y;
-  const int k = blockIdx.z;
-  if (ii >= g.NI) return;
   const long long p = off3(g, ii, jj, k);
   const int q = off2(g, ii, jj);
-  const double2* U = a.in;
-  auto V = [&](int v, int i2, int j2, int k2) { return ldf(U + (long long)v * g.fs, off3(g, i2, j2, k2)); };
   double2 r[5];
   const int n = g.NI - 1;
   if (jj <= 2 || jj >= g.NJ - 3 || k == 0 || k == g.Nz) {
@@ -102,50 +102,51 @@ __global__ void __launch_bounds__(128) cfg_stage_kernel(CfgArgs a) {
   } else if (ii == n) {
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      auto f = [&](int i2) { return V(v, i2, jj, k); };
-      r[v] = cneg(cadd(d4r(g, f, ii, a.rr), cdiv(V(v, ii, jj, k), a.rN)));
+      auto f = [&](int i2) { return S(v, i2, jj); };
+      r[v] = cneg(cadd(d4r(g, f, ii, a.rr), cdiv(S(v, ii, jj), a.rN)));
     }
   } else {
     const double al = ldm(M.alpha, q), b1 = ldm(M.beta, q), sg = ldm(M.sqrtg, q), dxb = ldm(a.dxb4, q);
     const int km2 = kper(g, k, -2), km1 = kper(g, k, -1), kp1 = kper(g, k, 1), kp2 = kper(g, k, 2);
-    auto E = [&](int i2, int j2, int k2) {
+    // alpha Pi + beta psi_1 on this plane (ES) and in the own column (EP)
+    auto ES = [&](int i2, int j2) {
       const int q2 = off2(g, i2, j2);
-      return cadd(rmul(ldm(M.alpha, q2), V(4, i2, j2, k2)), rmul(ldm(M.beta, q2), V(1, i2, j2, k2)));
+      return cadd(rmul(ldm(M.alpha, q2), S(4, i2, j2)), rmul(ldm(M.beta, q2), S(1, i2, j2)));
     };
-    auto Fp = [&](int j2, int k2) {
-      const int q2 = off2(g, ii, j2);
-      return rmul(ldm(M.asg, q2), cadd(rmul(ldm(M.grp, q2), V(1, ii, j2, k2)), rmul(ldm(M.gpp, q2), V(3, ii, j2, k2))));
+    auto EP = [&](int k2) { return cadd(rmul(ldm(M.alpha, q), P(4, k2)), rmul(ldm(M.beta, q), P(1, k2))); };
+    auto Fp = [&](int k2) {
+      return rmul(ldm(M.asg, q), cadd(rmul(ldm(M.grp, q), P(1, k2)), rmul(ldm(M.gpp, q), P(3, k2))));
     };
     // sqrt(gamma) carries the sign of sin(theta) through the pole: negative on the ghost rows
-    auto H = [&](int j2, int k2) {
-      const double2 h = rmul(ldm(M.asg_gtt, off2(g, ii, j2)), V(2, ii, j2, k2));
+    auto H = [&](int j2) {
+      const double2 h = rmul(ldm(M.asg_gtt, off2(g, ii, j2)), S(2, ii, j2));
       return (j2 <= 2 || j2 >= g.NJ - 3) ? cneg(h) : h;
     };
-    const double2 pi = V(4, ii, jj, k), ps1 = V(1, ii, jj, k);
+    const double2 pi = S(4, ii, jj), ps1 = S(1, ii, jj);
     r[0] = cadd(rmul(al, pi), rmul(b1, ps1));
     {
-      auto fA = [&](int i2) { return rmul(ldm(M.alpha, off2(g, i2, jj)), V(4, i2, jj, k)); };
-      auto fP = [&](int i2) { return V(1, i2, jj, k); };
+      auto fA = [&](int i2) { return rmul(ldm(M.alpha, off2(g, i2, jj)), S(4, i2, jj)); };
+      auto fP = [&](int i2) { return S(1, i2, jj); };
       r[1] = cadd(cadd(d4r(g, fA, ii, a.rr), rmul(b1, d4r(g, fP, ii, a.rr))), rmul(dxb, ps1));
     }
-    r[2] = d4c(E(ii, jj - 2, k), E(ii, jj - 1, k), E(ii, jj + 1, k), E(ii, jj + 2, k), a.rt);
-    r[3] = d4c(E(ii, jj, km2), E(ii, jj, km1), E(ii, jj, kp1), E(ii, jj, kp2), a.rp);
+    r[2] = d4c(ES(ii, jj - 2), ES(ii, jj - 1), ES(ii, jj + 1), ES(ii, jj + 2), a.rt);
+    r[3] = d4c(EP(km2), EP(km1), EP(kp1), EP(kp2), a.rp);
     {
       auto fG = [&](int i2) {
         const int q2 = off2(g, i2, jj);
-        return rmul(ldm(M.asg, q2), cadd(rmul(ldm(M.grr, q2), V(1, i2, jj, k)), rmul(ldm(M.grp, q2), V(3, i2, jj, k))));
+        return rmul(ldm(M.asg, q2), cadd(rmul(ldm(M.grr, q2), S(1, i2, jj)), rmul(ldm(M.grp, q2), S(3, i2, jj))));
       };
       auto fQ = [&](int i2) {
-        const double2 w = V(4, i2, jj, k);
+        const double2 w = S(4, i2, jj);
         const double s2 = ldm(M.sqrtg, off2(g, i2, jj));
         return c2(w.x * s2, w.y * s2);
       };
       const double2 t1 = cdiv(d4r(g, fG, ii, a.rr), sg);
-      const double2 t2 = cdiv(d4c(H(jj - 2, k), H(jj - 1, k), H(jj + 1, k), H(jj + 2, k), a.rt), sg);
-      const double2 t3 = cdiv(d4c(Fp(jj, km2), Fp(jj, km1), Fp(jj, kp1), Fp(jj, kp2), a.rp), sg);
+      const double2 t2 = cdiv(d4c(H(jj - 2), H(jj - 1), H(jj + 1), H(jj + 2), a.rt), sg);
+      const double2 t3 = cdiv(d4c(Fp(km2), Fp(km1), Fp(kp1), Fp(kp2), a.rp), sg);
       const double2 t4 = c2(pi.x * dxb, pi.y * dxb);
       const double2 t5 = cdiv(rmul(b1, d4r(g, fQ, ii, a.rr)), sg);
-      const double2 t6 = rmul(ldm(M.am2, q), V(0, ii, jj, k));
+      const double2 t6 = rmul(ldm(M.am2, q), S(0, ii, jj));
       r[4] = csub(cadd(cadd(cadd(cadd(t1, t2), t3), t4), t5), t6);
     }
     const int km3 = kper(g, k, -3), kp3 = kper(g, k, 3);
@@ -154,12 +155,12 @@ __global__ void __launch_bounds__(128) cfg_stage_kernel(CfgArgs a) {
     for (int v = 0; v < 5; ++v) {
       double2 s = r[v];
       if (kor)
-        s = cadd(s, rmul(a.kr, ko6(V(v, ii - 3, jj, k), V(v, ii - 2, jj, k), V(v, ii - 1, jj, k), V(v, ii, jj, k),
-                                   V(v, ii + 1, jj, k), V(v, ii + 2, jj, k), V(v, ii + 3, jj, k))));
-      s = cadd(s, rmul(a.kt, ko6(V(v, ii, jj - 3, k), V(v, ii, jj - 2, k), V(v, ii, jj - 1, k), V(v, ii, jj, k),
-                                 V(v, ii, jj + 1, k), V(v, ii, jj + 2, k), V(v, ii, jj + 3, k))));
-      s = cadd(s, rmul(a.kp, ko6(V(v, ii, jj, km3), V(v, ii, jj, km2), V(v, ii, jj, km1), V(v, ii, jj, k),
-                                 V(v, ii, jj, kp1), V(v, ii, jj, kp2), V(v, ii, jj, kp3))));
+        s = cadd(s, rmul(a.kr, ko6(S(v, ii - 3, jj), S(v, ii - 2, jj), S(v, ii - 1, jj), S(v, ii, jj),
+                                   S(v, ii + 1, jj), S(v, ii + 2, jj), S(v, ii + 3, jj))));
+      s = cadd(s, rmul(a.kt, ko6(S(v, ii, jj - 3), S(v, ii, jj - 2), S(v, ii, jj - 1), S(v, ii, jj),
+                                 S(v, ii, jj + 1), S(v, ii, jj + 2), S(v, ii, jj + 3))));
+      s = cadd(s, rmul(a.kp, ko6(P(v, km3), P(v, km2), P(v, km1), S(v, ii, jj), P(v, kp1), P(v, kp2),
+                                 P(v, kp3))));
       r[v] = s;
     }
   }
@@ -184,6 +185,77 @@ __global__ void __launch_bounds__(128) cfg_stage_kernel(CfgArgs a) {
       res = cadd(b, cdivr(cadd(a.acc[o], kk), 6.0));
     }
     a.out[o] = res;
+  }
+}
+
+// One thread per stored point; every neighbour through the read-only cache.
+template <int KIND>
+__global__ void __launch_bounds__(128) cfg_stage_kernel(CfgArgs a) {
+  const Grid& g = a.g;
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y;
+  const int k = blockIdx.z;
+  if (ii >= g.NI) return;
+  const double2* U = a.in;
+  auto S = [&](int v, int i2, int j2) { return ldf(U + (long long)v * g.fs, off3(g, i2, j2, k)); };
+  auto P = [&](int v, int k2) { return ldf(U + (long long)v * g.fs, off3(g, ii, jj, k2)); };
+  cfg_point<KIND>(a, ii, jj, k, S, P);
+}
+
+// Tiled form: a CTA owns a 32 x 8 tile of (r, theta) columns and marches through
+// a chunk of phi planes.  The plane being updated arrives in shared memory with
+// a +-4 r and +-3 theta halo (every same-plane neighbour the fourth-order
+// differences, the r closures and the sixth-order dissipation touch), double
+// buffered: the next plane's tile is copied by cp.async while this plane is
+// computed.  The phi neighbours of the thread's own column (planes k+-1..3)
+// are read through the read-only cache; the same values serve seven
+// consecutive planes of the march.
+constexpr int CTI = 32, CTJ = 8, CRH = 4, CTH = 3;
+constexpr int CW = CTI + 2 * CRH, CH = CTJ + 2 * CTH, CT_N = CW * CH;
+constexpr size_t CFG_TILE_BYTES = (size_t)5 * CT_N * sizeof(double2);
+
+template <int KIND>
+__global__ void __launch_bounds__(CTI * CTJ, 2) cfg_march_kernel(CfgArgs a, int kchunk) {
+  extern __shared__ __align__(16) unsigned char cfg_smem[];
+  double2* tiles = reinterpret_cast<double2*>(cfg_smem);
+  const Grid& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CTI + tx;
+  const int ii0 = blockIdx.x * CTI, jj0 = blockIdx.y * CTJ;
+  const int ii = ii0 + tx, jj = jj0 + ty;
+  const bool act = ii < g.NI && jj < g.NJ;
+  const int k0 = blockIdx.z * kchunk;
+  if (k0 >= g.NK) return;  // uniform over the block
+  const int k1 = min(k0 + kchunk, g.NK);
+  const double2* col = a.in + (act ? off3(g, ii, jj, 0) : 0);
+  // points of the halo tile outside the array are not copied; no stencil reads them
+  auto load = [&](int k, int buf) {
+    double2* dst = tiles + (size_t)buf * 5 * CT_N;
+    for (int t = tid; t < 5 * CT_N; t += CTI * CTJ) {
+      const int v = t / CT_N, r = t - v * CT_N, ly = r / CW, lx = r - ly * CW;
+      const int gi = ii0 - CRH + lx, gj = jj0 - CTH + ly;
+      if (gi >= 0 && gi < g.NI && gj >= 0 && gj < g.NJ)
+        cp_async16(dst + t, a.in + (long long)v * g.fs + off3(g, gi, gj, k));
+    }
+    cp_async_commit();
+  };
+  load(k0, 0);
+  for (int k = k0; k < k1; ++k) {
+    const int buf = (k - k0) & 1;
+    if (k + 1 < k1) {
+      load(k + 1, buf ^ 1);  // that buffer was last read before the previous block barrier
+      cp_async_wait_prior();
+    } else {
+      cp_async_wait_all();
+    }
+    __syncthreads();
+    if (act) {
+      // every same-plane neighbour lies inside the halo tile
+      const double2* T = tiles + (size_t)buf * 5 * CT_N + (ty + CTH) * CW + (tx + CRH);
+      auto S = [&](int v, int i2, int j2) { return T[v * CT_N + (j2 - jj) * CW + (i2 - ii)]; };
+      auto P = [&](int v, int k2) { return ldf(col + (long long)v * g.fs, (long long)k2 * g.plane); };
+      cfg_point<KIND>(a, ii, jj, k, S, P);
+    }
+    __syncthreads();
   }
 }
 
@@ -221,10 +293,36 @@ __global__ void cfg_ghost_rows(Grid g, double2* u) {
   }
 }
 
+template <int KIND>
+int cfg_march_launch(const CfgArgs& a, cudaStream_t st) {
+  static bool attr = false;  // dynamic shared memory above 48 KB, set once per stage kind
+  if (!attr) {
+    if (cudaFuncSetAttribute(cfg_march_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(2 * CFG_TILE_BYTES)) != cudaSuccess)
+      return -1;
+    attr = true;
+  }
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+  }
+  const Grid& g = a.g;
+  const int tx = (g.NI + CTI - 1) / CTI, ty = (g.NJ + CTJ - 1) / CTJ;
+  // about two waves of two CTAs per SM: small grids are cut into phi chunks
+  int nch = (4 * sms + tx * ty - 1) / (tx * ty);
+  nch = nch < 1 ? 1 : (nch > g.NK ? g.NK : nch);
+  const int kchunk = (g.NK + nch - 1) / nch;
+  nch = (g.NK + kchunk - 1) / kchunk;
+  cfg_march_kernel<KIND><<<dim3(tx, ty, nch), dim3(CTI, CTJ, 1), 2 * CFG_TILE_BYTES, st>>>(a, kchunk);
+  return 0;
+}
+
 }  // namespace
 
 int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, const double coef[6], double rN,
-                       cudaStream_t st) {
+                     int tiled, cudaStream_t st) {
   CfgArgs a;
   a.g = L.g;
   a.m = L.m;
@@ -240,6 +338,15 @@ int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, cons
   a.kt = coef[4];
   a.kp = coef[5];
   a.rN = rN;
+  if (tiled) {
+    switch (kind) {
+      case ST_RK4_1: return cfg_march_launch<ST_RK4_1>(a, st);
+      case ST_RK4_2: return cfg_march_launch<ST_RK4_2>(a, st);
+      case ST_RK4_3: return cfg_march_launch<ST_RK4_3>(a, st);
+      case ST_RK4_4: return cfg_march_launch<ST_RK4_4>(a, st);
+      default: return -1;
+    }
+  }
   dim3 grid((L.g.NI + 127) / 128, L.g.NJ, L.g.NK);
   switch (kind) {
     case ST_RK4_1: cfg_stage_kernel<ST_RK4_1><<<grid, 128, 0, st>>>(a); return 0;

@@ -84,9 +84,10 @@ void launch_ghost_fill_f32(const void* d_desc, int n, long long max_rows, long l
                            cudaStream_t st);
 // configured method (kg_config.cu): RK4 stage with fourth-order differences,
 // Kreiss-Oliger dissipation and a Sommerfeld outer plane; coef = 1/(12 h) for
-// r, theta, phi then eps/(64 h) for r, theta, phi; rN = outermost r
+// r, theta, phi then eps/(64 h) for r, theta, phi; rN = outermost r; tiled = 1
+// for the shared-memory tiled marching form, 0 for one thread per point (same bits)
 int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, const double coef[6], double rN,
-                     cudaStream_t st);
+                     int tiled, cudaStream_t st);
 void launch_ghost_fill_cfg(const Grid& g, double2* u, cudaStream_t st);
 // Berger-Oliger transfers between radially nested 2:1 levels (kg_refine.cu)
 int launch_prolong(const Grid& gf, double2* uf, const Grid& gc, const double2* c_old, const double2* c_new,

@@ -55,14 +55,6 @@ __host__ __device__ constexpr size_t mx_smem() {
   return (size_t)NST * slot_e<T>() * sizeof(T) + (size_t)MT_COUNT * MT_N * 8 + 64 + 128 +
          (sizeof(T) == 4 ? (size_t)STG_BYTES : 0);
 }
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(saddr(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // ---- a complex value in arithmetic type R -----------------------------------
 template <class R>

@@ -1,5 +1,5 @@
-// kg_tma_ops.cuh -- mbarrier and TMA (cp.async.bulk.tensor) primitives shared
-// by the TMA-pipelined stage kernels.  Waits are bounded: mbar_wait_bounded
+// kg_tma_ops.cuh -- mbarrier, TMA (cp.async.bulk.tensor) and cp.async primitives
+// shared by the pipelined stage kernels.  Waits are bounded: mbar_wait_bounded
 // returns false after WAIT_LIMIT polls so the caller can flag the error and
 // leave instead of spinning forever.  No multicast form is used.
 #pragma once
@@ -55,6 +55,17 @@ __device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap* tm, int c0, i
                : "memory");
 }
 
+// cp.async (LDGSTS) copies of 16 or 8 bytes into shared memory, grouped and waited per thread
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(saddr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// all but the most recently committed group have landed
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 }  // namespace tmaops
 }  // namespace kg

@@ -38,6 +38,22 @@ def test_configured_rk4_bitexact_vs_oracle(grid):
     assert np.array_equal(dev.u, ora.get_state())
 
 
+@pytest.mark.parametrize("grid", [(24, 17, 33), (67, 41, 9), (150, 9, 129)])
+def test_configured_tiled_equals_per_point(grid):
+    """the shared-memory tiled form (default) and the one-thread-per-point form
+    (kernel variant 0) give the same bits: partial tiles in r and theta, phi
+    chunks of one plane up to the whole range, and the oracle on the first grid"""
+    dev, ora = _pair(*grid, steps=3)
+    ref, _ = _pair(*grid, steps=3)
+    ref._ck(ref._lib.kg_set_kernel_variant(ref.handle, 0))
+    dev.rk4(nsteps=3)
+    ref.rk4(nsteps=3)
+    assert np.array_equal(dev.u, ref.u)
+    if grid == (24, 17, 33):
+        ora.rk4(3)
+        assert np.array_equal(dev.u, ora.get_state())
+
+
 def test_configured_scheme_guards():
     from kg_b200 import ScalarField, KgError
     s = ScalarField(16, 9, 17, 1.8, 12.0, 0.25)
