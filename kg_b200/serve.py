@@ -206,8 +206,11 @@ class Server:
             live = still + joined
             if not live:
                 if pending:
-                    raise RuntimeError("a single request exceeds the HBM budget")
-                if i_next < len(reqs):
+                    # admission ran before this quantum's retirements freed their memory;
+                    # the next pass admits unless the head request alone exceeds the budget
+                    if _bytes_estimate(pending[0], self.precision) > self.budget:
+                        raise RuntimeError("a single request exceeds the HBM budget")
+                elif i_next < len(reqs):
                     time.sleep(max(0.0, reqs[i_next].arrival - (time.perf_counter() - t0)))
         wall = time.perf_counter() - t0
         batch.close()

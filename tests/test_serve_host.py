@@ -1,0 +1,124 @@
+"""Host logic of the serving loop on the CPU: admission against the HBM budget,
+new arrivals prepared while a quantum runs and stepping from the next one,
+every waveform sample attributed to its own solve, retirement and clean-up.
+The device side (solves and the batched engine) is replaced by fakes that
+record what the loop asks of them."""
+import numpy as np
+import pytest
+
+
+class FakeSolve:
+    def __init__(self, req):
+        self.req = req
+        self.steps = 0
+        self.t = 0.0
+        self.closed = False
+
+    def close(self):
+        self.closed = True
+
+
+class FakeBatch:
+    instances = []
+
+    def __init__(self, device=-1, precision="fp64"):
+        self.members = []
+        self.in_flight = set()   # members queued in the running quantum
+        self.max_members = 0
+        self.closed = False
+        FakeBatch.instances.append(self)
+
+    def set_tuning(self, *a):
+        pass
+
+    def add(self, s):
+        assert s not in self.members
+        self.members.append(s)
+        self.max_members = max(self.max_members, len(self.members))
+
+    def remove(self, s):
+        self.members.remove(s)
+
+    def rk4(self, n):
+        self.in_flight = set(id(m) for m in self.members)
+        for m in self.members:
+            m.steps += n
+            m.t += n * 0.1
+            assert m.steps <= m.req.steps, "a solve stepped past its request"
+
+    def proyector_detectors(self):
+        # one (n_det, 2L+1, L+1) block per member; [0, 0, 0] encodes the solve and its step count
+        out = []
+        for m in self.members:
+            a = np.zeros((2, 3, 2), np.complex128)
+            a[0, 0, 0] = m.req.rid + 1j * m.steps
+            out.append(a)
+        return out
+
+    def close(self):
+        self.closed = True
+
+
+@pytest.fixture
+def served(monkeypatch):
+    import kg_b200.batch
+    import kg_b200.serve as serve
+    made = []
+
+    def make(req, l_max, device):
+        s = FakeSolve(req)
+        made.append(s)
+        return s
+
+    FakeBatch.instances.clear()
+    monkeypatch.setattr(serve, "_make_solve", make)
+    monkeypatch.setattr(kg_b200.batch, "Batch", FakeBatch)
+    return serve, made
+
+
+def test_batched_loop_attribution_and_cleanup(served):
+    serve, made = served
+    reqs = serve.draw_requests(seed=3, rate=1e6, count=40, nr=(16, 64), nr_step=16, ntheta=(8, 16),
+                               steps=(10, 120), quantum=10)
+    budget = 3.5 * max(serve._bytes_estimate(r) for r in reqs)
+    out = serve.Server(mode="batched", hbm_budget=budget, save_every=10).run(reqs)
+    assert out["completed"] == len(reqs)
+    b = FakeBatch.instances[-1]
+    assert b.closed and not b.members
+    assert all(s.closed for s in made) and len(made) == len(reqs)
+    assert out["peak_live"] >= 2               # requests overlapped
+    for res, r in zip(out["results"], sorted(reqs, key=lambda x: x.rid)):
+        assert res.rid == r.rid
+        samples = res.alm[:, 0, 0]
+        # one sample per quantum, each from this solve, the first after its first quantum:
+        # a solve that joined during a quantum did not take part in it
+        assert len(samples) == r.steps // 10
+        assert np.all(samples.real == r.rid)
+        assert np.array_equal(samples.imag, np.arange(10, r.steps + 1, 10))
+        assert np.allclose(res.times, 0.1 * np.arange(10, r.steps + 1, 10))
+
+
+def test_batched_loop_budget_never_exceeded(served, monkeypatch):
+    serve, made = served
+    reqs = serve.draw_requests(seed=4, rate=1e6, count=30, nr=(16, 96), nr_step=16, ntheta=(8, 16),
+                               steps=(10, 60), quantum=10)
+    budget = 2.2 * max(serve._bytes_estimate(r) for r in reqs)
+    live_bytes = []
+    orig_add = FakeBatch.add
+
+    def add(self, s):
+        orig_add(self, s)
+        live_bytes.append(sum(serve._bytes_estimate(m.req) for m in self.members))
+
+    monkeypatch.setattr(FakeBatch, "add", add)
+    out = serve.Server(mode="batched", hbm_budget=budget, save_every=10).run(reqs)
+    assert out["completed"] == len(reqs)
+    assert max(live_bytes) <= budget
+
+
+def test_request_larger_than_budget_is_refused(served):
+    serve, made = served
+    reqs = serve.draw_requests(seed=5, rate=1e6, count=2, nr=(64, 64), nr_step=16, ntheta=(16,),
+                               steps=(10, 10), quantum=10)
+    with pytest.raises(RuntimeError):
+        serve.Server(mode="batched", hbm_budget=serve._bytes_estimate(reqs[0]) / 2).run(reqs)
