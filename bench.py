@@ -411,10 +411,10 @@ def c0_leg(device, steps=1000):
 
 def refinement_leg(w, device, steps=10, r_fine=(20.0, 15.0, 10.0)):
     """The workload grid as the coarse level of a Berger-Oliger hierarchy with
-    radially nested 2:1 levels inside r < 20 (r_fine), FP64 RK4; level l takes
-    2^l steps per coarse step.  Rate = interior points x 4 stages x steps summed
-    over levels / device time (CUDA events on the coarse level's stream, which
-    every level's work is ordered back into)."""
+    radially nested 2:1 levels inside r < 20 (r_fine), FP64 RK4 and SSP-RK3;
+    level l takes 2^l steps per coarse step.  Rate = interior points x stages x
+    steps summed over levels / device time (CUDA events on the coarse level's
+    stream, which every level's work is ordered back into)."""
     import torch
     from kg_b200.refinement import BergerOliger
     from kg_b200.initial_data import shell_ylm_device
@@ -426,25 +426,28 @@ def refinement_leg(w, device, steps=10, r_fine=(20.0, 15.0, 10.0)):
         lv._ck(lv._lib.kg_set_state_device(lv.handle, 0, C.c_void_p(u0.data_ptr())))
         lv.synchronize()
         del u0
-    bo.rk4(1)
-    bo.synchronize()
     l0 = bo.levels[0]
     stream = torch.cuda.ExternalStream(l0._lib.kg_get_stream(l0.handle), device=f"cuda:{device}")
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    bo.rk4(steps)
-    e1.record(stream)
-    e1.synchronize()
-    bo.synchronize()
-    ms = e0.elapsed_time(e1)
-    work = sum(lv.Nx * (lv.Ny - 1) * (lv.Nz - 1) * 4 * (2 ** l) for l, lv in enumerate(bo.levels)) * steps
+    out = {"workload": f"coarse level = the workload grid; 2:1 levels inside r < {r_fine}, {steps} coarse steps "
+                       f"per stepper",
+           "levels": [{"Nx": lv.Nx, "r_outer": lv.params.xmax, "dt": lv.dt} for lv in bo.levels]}
+    for method, stages in (("rk4", 4), ("rk3", 3)):
+        getattr(bo, method)(1)
+        bo.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        getattr(bo, method)(steps)
+        e1.record(stream)
+        e1.synchronize()
+        bo.synchronize()
+        ms = e0.elapsed_time(e1)
+        work = sum(lv.Nx * (lv.Ny - 1) * (lv.Nz - 1) * stages * (2 ** l) for l, lv in enumerate(bo.levels)) * steps
+        out[method] = {"ms_per_coarse_step": ms / steps, "gpsu": work / (ms / 1e3)}
     finite = True
     for lv in bo.levels:
         lv.density()
         finite = finite and bool(np.isfinite(lv.mass_scalar()))
-    out = {"workload": f"coarse level = the workload grid; 2:1 levels inside r < {r_fine}, RK4, {steps} coarse steps",
-           "levels": [{"Nx": lv.Nx, "r_outer": lv.params.xmax, "dt": lv.dt} for lv in bo.levels],
-           "ms_per_coarse_step": ms / steps, "gpsu": work / (ms / 1e3), "finite": finite}
+    out["finite"] = finite
     bo.close()
     return out
 

@@ -273,6 +273,9 @@ const char *kg_hier_last_error(const kg_hier *H);
 int kg_hier_levels(const kg_hier *H);
 kg_solver *kg_hier_level(kg_hier *H, int level);
 int kg_hier_rk4(kg_hier *H, int coarse_steps);
+/* the same hierarchy stepped by SSP-RK3 (rk3, MoL/lines_method_lib.f90:211-269);
+ * the stage inputs stand at t, t+dt and t+dt/2 for the buffer-plane times */
+int kg_hier_rk3(kg_hier *H, int coarse_steps);
 int kg_hier_synchronize(kg_hier *H);
 
 /* --- allocation-free diagnostic --------------------------------------------- */

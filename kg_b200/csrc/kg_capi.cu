@@ -1183,6 +1183,43 @@ int step_rk4_bo(kg_solver* h, kg_solver* c, const double2* c_old, double a0, dou
   return KG_OK;
 }
 
+// SSP-RK3 step of a refined level (rk3, MoL/lines_method_lib.f90:211-269): the
+// stage inputs u, u1 = u + dt L(u) and u2 = 3/4 u + 1/4 (u1 + dt L(u1)) stand
+// at t, t + dt and t + dt/2, so each stage output's buffer planes take the
+// coarse values interpolated to those times.
+int step_rk3_bo(kg_solver* h, kg_solver* c, const double2* c_old, double a0, double da, int nbuf) {
+  int rc;
+  if ((rc = ensure(h, &h->RK, 15))) return rc;
+  const Grid& g = h->g;
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  double2* R1 = h->RK;
+  double2* R2 = fld(h->RK, g, 5);
+  auto prolong = [&](double2* u, double alpha) -> int {
+    Prof pf(h, PK_PROLONG, 1);
+    if (kg::launch_prolong(g, u, c->g, c_old, c->U, alpha, nbuf, h->stream))
+      return set_err(h, KG_EINVAL, "refined level does not fit inside its coarser level");
+    return KG_OK;
+  };
+  if ((rc = prolong(h->U, a0))) return rc;
+  kg::StageLaunch L = base_launch(h);
+  L.base = h->U;
+  double2* ins[3] = {h->U, R1, R2};
+  double2* outs[3] = {R1, R2, h->U};
+  const int kinds[3] = {kg::ST_RK3_1, kg::ST_RK3_2, kg::ST_RK3_3};
+  const double at[3] = {a0 + da, a0 + 0.5 * da, a0 + da};
+  for (int st = 0; st < 3; ++st) {
+    set_in(L, g, ins[st], fld(ins[st], g, 4));
+    L.out = outs[st];
+    L.skip_last_i = (st == 2) ? inflow : 0;
+    run_stage(h, kinds[st], L);
+    run_ghost(h, outs[st], h->U, inflow);
+    if ((rc = prolong(outs[st], at[st]))) return rc;
+  }
+  h->t = h->t + h->dt;
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
 // Runs nsteps steps.  Pairs of steps are replayed from a CUDA graph captured
 // once per stepper and Pi-slot state (two steps return the PIRK slots to the
 // state they started in); an odd last step, or runs with profiling on, launch
@@ -2263,7 +2300,8 @@ int hier_order(kg_hier* H, kg_solver* from, kg_solver* to, int l) {
   return KG_OK;
 }
 
-int hier_step(kg_hier* H, int l, double a0, double da) {
+// method: 3 = SSP-RK3, 4 = RK4 on every level
+int hier_step(kg_hier* H, int l, double a0, double da, int method) {
   kg_solver* h = H->lv[l];
   const int n = (int)H->lv.size();
   int rc;
@@ -2273,7 +2311,8 @@ int hier_step(kg_hier* H, int l, double a0, double da) {
       return KG_ECUDA;
     }
   }
-  if (l == 0) rc = step_rk4(h, 1);
+  if (l == 0) rc = method == 3 ? step_rk3(h, 1) : step_rk4(h, 1);
+  else if (method == 3) rc = step_rk3_bo(h, H->lv[l - 1], H->uold[l - 1], a0, da, H->nbuf);
   else rc = step_rk4_bo(h, H->lv[l - 1], H->uold[l - 1], a0, da, H->nbuf);
   if (rc) {
     H->err = h->err;
@@ -2283,7 +2322,7 @@ int hier_step(kg_hier* H, int l, double a0, double da) {
     kg_solver* f = H->lv[l + 1];
     if ((rc = hier_order(H, h, f, l))) return rc;
     for (int sub = 0; sub < 2; ++sub)
-      if ((rc = hier_step(H, l + 1, 0.5 * sub, 0.5))) return rc;
+      if ((rc = hier_step(H, l + 1, 0.5 * sub, 0.5, method))) return rc;
     if ((rc = hier_order(H, f, h, l))) return rc;
     Prof pf(h, PK_RESTRICT, 1);
     if (kg::launch_restrict(h->g, h->U, f->g, f->U, H->keep_out, h->stream)) {
@@ -2374,7 +2413,8 @@ kg_solver* kg_hier_level(kg_hier* H, int l) {
 }
 
 // nsteps coarse steps of RK4 (MoL/lines_method_lib.f90:411-474) on every level
-int kg_hier_rk4(kg_hier* H, int nsteps) {
+namespace {
+int hier_run(kg_hier* H, int nsteps, int method) {
   if (!H || nsteps < 0) return KG_EINVAL;
   for (kg_solver* h : H->lv)
     if (h->scheme != 0 || h->precision != 0) {
@@ -2382,12 +2422,16 @@ int kg_hier_rk4(kg_hier* H, int nsteps) {
       return KG_EINVAL;
     }
   for (int s = 0; s < nsteps; ++s) {
-    const int rc = hier_step(H, 0, 0.0, 1.0);
+    const int rc = hier_step(H, 0, 0.0, 1.0, method);
     if (rc) return rc;
     H->coarse_steps++;
   }
   return KG_OK;
 }
+}  // namespace
+
+int kg_hier_rk4(kg_hier* H, int nsteps) { return hier_run(H, nsteps, 4); }
+int kg_hier_rk3(kg_hier* H, int nsteps) { return hier_run(H, nsteps, 3); }
 
 int kg_hier_synchronize(kg_hier* H) {
   if (!H) return KG_EINVAL;

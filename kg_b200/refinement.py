@@ -77,6 +77,10 @@ class BergerOliger:
         """nsteps coarse RK4 steps (level l takes 2^l steps per coarse step)"""
         self._ck(self._lib.kg_hier_rk4(self._H, int(nsteps)))
 
+    def rk3(self, nsteps=1):
+        """nsteps coarse SSP-RK3 steps (level l takes 2^l steps per coarse step)"""
+        self._ck(self._lib.kg_hier_rk3(self._H, int(nsteps)))
+
     def synchronize(self):
         self._ck(self._lib.kg_hier_synchronize(self._H))
 
