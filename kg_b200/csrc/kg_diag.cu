@@ -84,23 +84,39 @@ void launch_density(const Grid& g, const Metric& m, const double2* u, double mas
 // trapezium over i in [0,Nx] (ii in [2, NI-3]), j in [0,Ny], k in [0,Nz] of
 // rho*sqrtg, weights 1/2 on the first and last index of each direction
 static const int MASS_THREADS = 256;
-int mass_blocks(const Grid& g) { return 148 * 4; }
+int mass_blocks(const Grid& g) { return 148 * 8; }
 
+// Each warp takes whole (theta, phi) rows in turn and its lanes stride along r
+// with four independent loads in flight, so the loads are coalesced and no
+// per-point index division is needed; the block count is fixed, so the partial
+// sums (and the result) do not depend on the device.
 __global__ void mass_partial_kernel(Grid g, const double* __restrict__ sqrtg, const double* __restrict__ rho,
                                     double* partials) {
   const int ni = g.NI - 4, nj = g.NJ - 4, nk = g.NK;
-  const long long n = (long long)ni * nj * nk;
+  const int rows = nj * nk;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   double acc = 0.0;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const int a = (int)(t % ni);
-    const long long r = t / ni;
-    const int b = (int)(r % nj), k = (int)(r / nj);
-    const int ii = a + 2, jj = b + 2;
-    double w = 1.0;
-    if (a == 0 || a == ni - 1) w *= 0.5;
-    if (b == 0 || b == nj - 1) w *= 0.5;
-    if (k == 0 || k == nk - 1) w *= 0.5;
-    acc += w * (rho[off3(g, ii, jj, k)] * sqrtg[off2(g, ii, jj)]);
+  for (int row = blockIdx.x * nw + (threadIdx.x >> 5); row < rows; row += gridDim.x * nw) {
+    const int b = row % nj, k = row / nj;
+    const int jj = b + 2;
+    double wjk = 1.0;
+    if (b == 0 || b == nj - 1) wjk *= 0.5;
+    if (k == 0 || k == nk - 1) wjk *= 0.5;
+    const double* rr = rho + off3(g, 2, jj, k);
+    const double* sr = sqrtg + off2(g, 2, jj);
+    for (int a0 = lane; a0 < ni; a0 += 128) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int a = a0 + 32 * u;
+        const double w = (a == 0 || a == ni - 1) ? 0.5 * wjk : wjk;
+        v[u] = a < ni ? w * (__ldg(rr + a) * __ldg(sr + a)) : 0.0;
+      }
+      acc += v[0];
+      acc += v[1];
+      acc += v[2];
+      acc += v[3];
+    }
   }
   acc = block_sum(acc);
   if (threadIdx.x == 0) partials[blockIdx.x] = acc;

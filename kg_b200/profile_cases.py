@@ -4,6 +4,7 @@
     python -m kg_b200.profile_cases configured [--grid Nx,Ny,Nz] [--steps K]
     python -m kg_b200.profile_cases batch      [--solves N] [--precision fp64|mixed] [--mix serving|c3] [--steps K]
     python -m kg_b200.profile_cases refine     [--grid Nx,Ny,Nz] [--steps K]
+    python -m kg_b200.profile_cases diag       [--grid Nx,Ny,Nz] [--steps K]
 
 Each case builds seeded synthetic input on the device, runs K steps and exits
 0 (or raises); the sizes default to a few GB of device memory, larger than
@@ -15,6 +16,9 @@ L2, so a profiler capture of one launch is representative and ends quickly.
               mix (Nr 128..512, Ntheta 16/32) or the batching-form mix
               (Nr 128..1024, Ntheta 16/32/64)
   refine:     a two-level Berger-Oliger hierarchy (prolong/restrict kernels)
+  diag:       the diagnostics of the evolve loop K times: density, the mass
+              integral (warp-shuffle partial sums), the currents and the
+              detector projection
 """
 from __future__ import annotations
 
@@ -36,7 +40,7 @@ def _device_ic(s, Nx, Ny, Nz, xmin, xmax, seed=7):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["mixed", "configured", "batch", "refine"])
+    ap.add_argument("case", choices=["mixed", "configured", "batch", "refine", "diag"])
     ap.add_argument("--grid", default=None)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--solves", type=int, default=30)
@@ -81,6 +85,17 @@ def main(argv=None):
         for _ in range(a.steps):
             b.rk4(1)
         b.synchronize()
+    elif a.case == "diag":
+        Nx, Ny, Nz = _grid(a.grid, (512, 129, 257))
+        xmax = 1.8 + 0.1944 * Nx
+        s = ScalarField(Nx, Ny, Nz, 1.8, xmax, 0.25, m=0.3, l_max=8, n_det=5, device=0)
+        _device_ic(s, Nx, Ny, Nz, 1.8, xmax)
+        for _ in range(a.steps):
+            s.density()
+            s.mass_scalar()
+            s.currents_detectors()
+            s.proyector_detectors()
+        s.synchronize()
     else:
         from .refinement import BergerOliger
         Nx, Ny, Nz = _grid(a.grid, (512, 65, 129))
