@@ -105,11 +105,15 @@ def test_steppers_bitexact(method, metric, bc, variant):
 
 
 @pytest.mark.parametrize("grid", [SMALL, dict(Nx=61, Ny=13, Nz=41, xmin=1.8, xmax=30.0),
-                                  dict(Nx=40, Ny=12, Nz=9, xmin=1.8, xmax=20.0)])
+                                  dict(Nx=40, Ny=12, Nz=9, xmin=1.8, xmax=20.0),
+                                  dict(Nx=4, Ny=5, Nz=5, xmin=1.8, xmax=6.0),
+                                  dict(Nx=12, Ny=7, Nz=8, xmin=1.8, xmax=9.0)])
 @pytest.mark.parametrize("variant", [1, 2])
 def test_march_ragged_tiles(grid, variant):
     """Grids whose r, theta and phi extents leave partial tiles and chunks
-    (including a last theta tile of one row) stay bit-exact."""
+    (including a last theta tile of one row) stay bit-exact; the smallest grid
+    kg_create accepts (Nx = 4, Ny = Nz = 5) and an even Nz, whose pole partner
+    plane k + Nz/2 is not a half turn (the reference's index rule), included."""
     dev, ora = _pair(grid=grid)
     dev._ck(dev._lib.kg_set_kernel_variant(dev.handle, variant))
     from kg_b200.initial_data import shell_ylm
