@@ -53,7 +53,7 @@ constexpr int STG_BYTES = TI * TJ * 5 * (16 + 8);
 template <class T>
 __host__ __device__ constexpr size_t mx_smem() {
   return (size_t)NST * slot_e<T>() * sizeof(T) + (size_t)MT_COUNT * MT_N * 8 + 64 + 128 +
-         (sizeof(T) == 4 ? (size_t)STG_BYTES : 0);
+         (sizeof(T) == 4 ? (size_t)STG_BYTES + (size_t)MT_COUNT * MT_N * 4 : 0);
 }
 
 // ---- a complex value in arithmetic type R -----------------------------------
@@ -130,9 +130,9 @@ namespace {
 // RHS of all five variables at the thread's own point, arithmetic in R.
 // cu: ring slot of plane k; E/F: phi-derivative arguments at k-1 and k+1.
 template <class R, int MK, class TIN>
-__device__ __forceinline__ void mx_rhs(const MxArgs& a, const TIN* cu, const double* mt, int tx, int ty, int ii,
-                                       int jj, int k, const double* own, double2 Epv, double2 Enx, double2 Fpv,
-                                       double2 Fnx, cx<R> r[5]) {
+__device__ __forceinline__ void mx_rhs(const MxArgs& a, const TIN* cu, const double* mt, const float* mtf, int tx,
+                                       int ty, int ii, int jj, int k, const double* own, double2 Epv, double2 Enx,
+                                       double2 Fpv, double2 Fnx, cx<R> r[5]) {
   const Grid& g = a.g;
   const Metric& M = a.m;
   const TIN* gin = reinterpret_cast<const TIN*>(a.in);
@@ -142,7 +142,13 @@ __device__ __forceinline__ void mx_rhs(const MxArgs& a, const TIN* cu, const dou
   auto RF = [&](int f, int dx, int dy) -> cx<R> {
     return ld2<R>(cu + (size_t)f * FIELD_E + (dy + 1) * RW + 2 * (dx + RH));
   };
-  auto MTV = [&](int which, int dx, int dy) -> R { return (R)mt[which * MT_N + (dy + 1) * MW + dx + RH]; };
+  // metric at tile point (dx, dy); the FP32 arithmetic reads the FP32 copy of the
+  // tile where there is one (stages with an FP32 ring), without a conversion per use
+  auto MTV = [&](int which, int dx, int dy) -> R {
+    const int o = which * MT_N + (dy + 1) * MW + dx + RH;
+    if (sizeof(R) == 4 && sizeof(TIN) == 4) return (R)mtf[o];
+    return (R)mt[o];
+  };
   auto G = [&](int v, long long p) -> cx<R> { return ld2<R>(gin + 2 * ((long long)v * g.fs + p)); };
   cx<R> fcu[5];
 #pragma unroll
@@ -255,6 +261,8 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
   constexpr bool STG = sizeof(TIN) == 4;
   double2* base_s = reinterpret_cast<double2*>(stg);
   float2* acc_s = reinterpret_cast<float2*>(stg + (size_t)TI * TJ * 5 * 16);
+  // FP32 copy of the metric tile (stages with an FP32 ring; it sits after the FP64 tile)
+  float* mtf = reinterpret_cast<float*>(mt + (size_t)MT_COUNT * MT_N);
   const Grid& g = a.g;
   const Metric& M = a.m;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TI + tx;
@@ -299,6 +307,8 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
     mt[MT_GRP * MT_N + t] = in ? ldm(M.grp, q) : 0.0;
     mt[MT_SG * MT_N + t] = in ? ldm(M.sqrtg, q) : 0.0;
     mt[MT_HT * MT_N + t] = in ? ldm(M.asg_gtt, q) : 0.0;
+    if (STG)
+      for (int w = 0; w < MT_COUNT; ++w) mtf[w * MT_N + t] = (float)mt[w * MT_N + t];
   }
   __syncthreads();
   auto prefetch = [&](int k) {
@@ -386,12 +396,12 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
       double2 rr[5];
       if (hp) {
         cx<double> r[5];
-        mx_rhs<double, MK, TIN>(a, cu, mt, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
+        mx_rhs<double, MK, TIN>(a, cu, mt, mtf, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
 #pragma unroll
         for (int v = 0; v < 5; ++v) rr[v] = make_double2(r[v].x, r[v].y);
       } else {
         cx<float> r[5];
-        mx_rhs<float, MK, TIN>(a, cu, mt, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
+        mx_rhs<float, MK, TIN>(a, cu, mt, mtf, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
 #pragma unroll
         for (int v = 0; v < 5; ++v) rr[v] = make_double2((double)r[v].x, (double)r[v].y);
       }
@@ -478,7 +488,8 @@ __global__ void __launch_bounds__(TI * TJ, 2)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TIN* ring = reinterpret_cast<TIN*>(align128(smem_raw));
   double* mt = reinterpret_cast<double*>(ring + (size_t)NST * slot_e<TIN>());
-  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(mt + (size_t)MT_COUNT * MT_N) +
+                                               (sizeof(TIN) == 4 ? (size_t)MT_COUNT * MT_N * 4 : 0));
   unsigned char* stg = reinterpret_cast<unsigned char*>(bars + 8);
   if ((int)blockIdx.z * a.kchunk >= a.g.NK) return;
   init_bars(bars);
@@ -491,7 +502,8 @@ __global__ void __launch_bounds__(TI * TJ, 2) mx_batch_kernel(const MxItem* __re
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TIN* ring = reinterpret_cast<TIN*>(align128(smem_raw));
   double* mt = reinterpret_cast<double*>(ring + (size_t)NST * slot_e<TIN>());
-  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(mt + (size_t)MT_COUNT * MT_N) +
+                                               (sizeof(TIN) == 4 ? (size_t)MT_COUNT * MT_N * 4 : 0));
   unsigned char* stg = reinterpret_cast<unsigned char*>(bars + 8);
   __shared__ MxArgs sa;
   __shared__ int s_bx, s_by, s_bz, s_solve;
