@@ -17,7 +17,11 @@
 //     correctly rounded quotient a/b when y = RN(1/b) and q = RN(a y)
 //     (P. Markstein, IBM J. Res. Dev. 34 (1990); Muller et al., Handbook of
 //     Floating-Point Arithmetic, the theorem on division by a correctly rounded
-//     reciprocal), so results equal IEEE division.
+//     reciprocal), so results equal IEEE division while the residual a - b q
+//     stays normal: for dividends below about 2^-1000 in magnitude (a field
+//     tail on its way to underflow) the quotient can be one unit off.  A guard
+//     that divides outright there cost the PIRK2 step 9 %; the per-point form
+//     (kg_stencil.cu) divides outright everywhere.
 // Stencils at the array ends, the theta pole row (partner plane k + Nz/2) and
 // the phi seam planes follow the reference exactly; values that fall outside
 // the tile are computed directly from global memory.

@@ -17,7 +17,8 @@
 //     with a per-CTA metric tile that is loaded once (the metric is
 //     phi-independent);
 //   * divisions by sqrt(gamma) use the correctly rounded host reciprocal and
-//     one Markstein step (see kg_march.cu), equal to IEEE division.
+//     one Markstein step (see kg_march.cu), equal to IEEE division for
+//     dividends above about 2^-1000 in magnitude.
 // All TMA coordinates are multiples of 16 bytes in x (the r axis is addressed
 // in doubles, two per complex value) and the boxes start at most 2 points
 // before the array or one row above it, where the loads read zeros.  Waits on

@@ -44,6 +44,25 @@ def test_metric_tables_match_oracle():
         assert dev.validate_inverse_metric() == (0, 0)
 
 
+def test_values_next_to_underflow_per_point_form():
+    """A field scaled to ~1e-303, the size a Gaussian tail passes through on its
+    way to underflow.  The per-point form (kernel variant 0) divides by
+    sqrt(gamma) outright and stays bit-exact with the oracle here.  The tiled
+    forms divide by a reciprocal product with one Markstein correction, which
+    can differ from IEEE division by one unit in the last place for dividends
+    below about 2^-1000, a relative error far inside the parity bound."""
+    dev, ora = _pair()
+    dev._ck(dev._lib.kg_set_kernel_variant(dev.handle, 0))
+    u0 = _ic() * 1e-303
+    assert 0 < np.abs(u0).max() < 1e-301
+    dev.u = u0
+    ora.set_state(u0)
+    for method in ("pirk2", "pirk2", "rk4", "pirk3"):
+        getattr(dev, method)()
+        ora.step(method, 1)
+        assert np.array_equal(dev.u, ora.get_state()), method
+
+
 def test_state_roundtrip():
     dev, _ = _pair()
     u = _ic()
