@@ -172,7 +172,6 @@ int kg_diagnostic(kg_solver *h, int index, double *mass_out);
 /* replace the detector radii (the reference places them at MoL/diagnostic_lib.f90:124-134);
  * each radius is located on the vertex grid the same way (main/global_numbers.f90:152-164) */
 int kg_set_detectors(kg_solver *h, int n, const double *radii);
-/* detector radii and vertex indices (1-based) */
 /* check_point / read_from_check_point (MoL/lines_method_lib.f90:599-667), as a
  * complete binary file: a 128-byte header (magic "KGB2CKPT", version, grid
  * integers, metric, outer BC, scheme, precision, t, dt, ...), then u and, when
@@ -183,6 +182,7 @@ int kg_set_detectors(kg_solver *h, int n, const double *radii);
  * reader deletes the file before opening it). */
 int kg_save_checkpoint(kg_solver *h, const char *path);
 int kg_load_checkpoint(kg_solver *h, const char *path);
+/* detector radii and vertex indices (1-based) */
 int kg_get_detectors(kg_solver *h, double *r_det, int *index_det);
 /* proyector_detectors applied at every vertex shell r(1..Nx) (tools/FFT_sph.f90:247-279
  * at all radii): alm(l, m, shell) complex, l fastest, m = -L..L, then shell.
@@ -217,7 +217,12 @@ const char *kg_profile_kind_name(int kind);
 long long kg_launch_count(const kg_solver *h);
 /* stage-kernel form: 2 = marching kernels fed by a TMA shared-memory ring
  * (default), 1 = 2.5-D marching kernels with register prefetch, 0 = one thread
- * per point with cached neighbour loads; all give bit-identical results */
+ * per point with cached neighbour loads; all give bit-identical results,
+ * except that forms 1 and 2 divide by sqrt(gamma) through a reciprocal
+ * product that can be one unit off IEEE division for dividends below about
+ * 2^-1000 in magnitude (form 0 divides outright).  The configured method
+ * (kg_set_scheme) takes 0 for one thread per point and any other value for
+ * its tiled form, which gives the same bits. */
 int kg_set_kernel_variant(kg_solver *h, int variant);
 
 /* --- batched engine ------------------------------------------------------------ */
