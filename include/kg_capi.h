@@ -287,10 +287,9 @@ int kg_hier_synchronize(kg_hier *H);
 
 /* Mass_scalar = integrate(rho*sqrtg) without allocating anything.  No
  * counterpart in the reference: it exists for callers that cannot call
- * cudaMalloc -- a host that records its time loop into a CUDA graph (an
- * allocation inside a stream capture breaks the capture) or whose device
- * memory belongs to its own pool or a fixed budget already given to live
- * solves.  The caller passes everything in its own device memory: rho as
+ * cudaMalloc -- a host whose device memory belongs to its own pool or a fixed
+ * budget already given to live solves, or one that must not take the
+ * device-wide synchronisation of cudaMalloc / cudaFree inside its time loop.  The caller passes everything in its own device memory: rho as
  * (Nz+1) x (Ny+2g+1) x (Nx+2g+1) doubles (r fastest, ghosts included, g = 2),
  * sqrtg as (Ny+2g+1) x (Nx+2g+1), and one double for the result; the work is
  * enqueued on `stream` (a cudaStream_t, NULL for the default stream) and the

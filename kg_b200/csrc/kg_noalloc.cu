@@ -3,10 +3,10 @@
 //
 // kg_mass_scalar() reduces into partial sums that live in device memory owned
 // by a solver handle, and the handle itself is created with cudaMalloc.  Some
-// callers cannot do that: a host that records its time loop into a CUDA graph
-// (cudaMalloc / cudaFree inside a stream capture invalidate it), or a host
-// whose device memory is all owned by its own pool allocator or already
-// committed to live solves under a fixed budget.  kg_integrate_mass_noalloc()
+// callers cannot do that: a host whose device memory is all owned by its own
+// pool allocator or already committed to live solves under a fixed budget, or
+// one that must not take the device-wide synchronisation cudaMalloc and
+// cudaFree imply in the middle of its time loop.  kg_integrate_mass_noalloc()
 // gives them the same diagnostic with no allocation at all: the caller passes
 // the density, the sqrt(gamma) table and an output slot, all in its own device
 // memory, and the intermediate sums go to one file-scope __device__ array.

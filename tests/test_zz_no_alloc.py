@@ -1,6 +1,7 @@
 """GPU test of kg_integrate_mass_noalloc, the mass integral for callers that
-cannot allocate device memory (a host recording its loop into a CUDA graph,
-or one whose device memory is owned by its own pool or budget).
+cannot allocate device memory (a host whose device memory is owned by its own
+pool or a fixed budget, or one that must not take the device-wide
+synchronisation of cudaMalloc / cudaFree inside its time loop).
 
 The entry point is called through the C ABI on device buffers the test owns,
 twice in a row on different densities, and each result is checked against
