@@ -290,6 +290,123 @@ class NumpyKG:
             self.boundary()
         self.t += dt
 
+    # ---- the configured method: fourth-order differences, sixth-order
+    # Kreiss-Oliger dissipation, Sommerfeld outer plane, RK4, Kerr-Schild form.
+    # The reference wires only second-order operators; this restates the C
+    # oracle's definition of the method (oracle/kg_oracle.c, rhs_cfg,
+    # boundary_cfg, rk4_cfg) in array form, with the one-sided closures of
+    # first_derivative_x_4 (tools/finite_differences.f90:124-154) on the first
+    # and last two r planes.
+    def set_scheme_cfg(self, ko_eps=0.02):
+        if self.metric != "Kerr_Schild":
+            raise ValueError("the configured method is written for the Kerr-Schild form")
+        self.ko_eps = ko_eps
+        F = self.beta[0]
+        res = 1.0 / (12.0 * self.dx)
+        n = F.shape[0] - 1
+        D = np.empty_like(F)
+        D[0] = (-25.0 * F[0] + 48.0 * F[1] - 36.0 * F[2] + 16.0 * F[3] - 3.0 * F[4]) * res
+        D[1] = (-3.0 * F[0] - 10.0 * F[1] + 18.0 * F[2] - 6.0 * F[3] + 1.0 * F[4]) * res
+        D[2:n - 1] = (F[0:n - 3] - 8.0 * F[1:n - 2] + 8.0 * F[3:n] - F[4:n + 1]) * res
+        D[n - 1] = (3.0 * F[n] + 10.0 * F[n - 1] - 18.0 * F[n - 2] + 6.0 * F[n - 3] - 1.0 * F[n - 4]) * res
+        D[n] = (25.0 * F[n] - 48.0 * F[n - 1] + 36.0 * F[n - 2] - 16.0 * F[n - 3] + 3.0 * F[n - 4]) * res
+        self.dx_beta4 = D
+
+    @staticmethod
+    def d4r(F, res):
+        """fourth-order r derivative of an array (r first), closures on two planes per end"""
+        D = np.empty_like(F)
+        n = F.shape[0] - 1
+        D[0] = -25.0 * F[0] + 48.0 * F[1] - 36.0 * F[2] + 16.0 * F[3] - 3.0 * F[4]
+        D[1] = -3.0 * F[0] - 10.0 * F[1] + 18.0 * F[2] - 6.0 * F[3] + 1.0 * F[4]
+        D[2:n - 1] = F[0:n - 3] - 8.0 * F[1:n - 2] + 8.0 * F[3:n] - F[4:n + 1]
+        D[n - 1] = 3.0 * F[n] + 10.0 * F[n - 1] - 18.0 * F[n - 2] + 6.0 * F[n - 3] - 1.0 * F[n - 4]
+        D[n] = 25.0 * F[n] - 48.0 * F[n - 1] + 36.0 * F[n - 2] - 16.0 * F[n - 3] + 3.0 * F[n - 4]
+        return D * res
+
+    @staticmethod
+    def d4c(fm2, fm1, fp1, fp2, res):
+        return (fm2 - 8.0 * fm1 + 8.0 * fp1 - fp2) * res
+
+    @staticmethod
+    def ko6(m3, m2, m1, c0, p1, p2, p3):
+        return m3 - 6.0 * m2 + 15.0 * m1 - 20.0 * c0 + 15.0 * p1 - 6.0 * p2 + p3
+
+    def rhs_cfg(self, v):
+        NI, NJ, Nz = self.NI, self.NJ, self.Nz
+        rr, rt, rp = 1.0 / (12.0 * self.dx), 1.0 / (12.0 * self.dy), 1.0 / (12.0 * self.dz)
+        kr, kt, kp = (self.ko_eps / (64.0 * h) for h in (self.dx, self.dy, self.dz))
+        b = self._b
+        al, b1, sg, dxb = b(self.alpha), b(self.beta[0]), b(self.sqrtg), b(self.dx_beta4)
+        asg = b(self.alpha * self.sqrtg)
+        gu = self.gamma_up
+        n = NI - 1
+        I, J, K = slice(0, n), slice(3, NJ - 3), slice(1, Nz)   # points with the full RHS
+        ks = np.arange(1, Nz)
+        kper = lambda d: ((ks - 1 + d) % (Nz - 1)) + 1
+        jsh = lambda d: slice(3 + d, NJ - 3 + d)
+        out = np.zeros_like(v)
+        # Sommerfeld plane: d_t u = -(d_r u + u / r)
+        rN = self.x[-1]
+        for w in range(5):
+            out[w, n, J, K] = -(self.d4r(v[w], rr)[n, J, K] + self.cdiv(v[w, n, J, K], rN))
+        E = al * v[4] + b1 * v[1]
+        r = [None] * 5
+        r[0] = E[I, J, K]
+        r[1] = (self.d4r(al * v[4], rr) + b1 * self.d4r(v[1], rr) + dxb * v[1])[I, J, K]
+        r[2] = self.d4c(E[:, jsh(-2)], E[:, jsh(-1)], E[:, jsh(1)], E[:, jsh(2)], rt)[I, :, K]
+        r[3] = self.d4c(E[:, :, kper(-2)], E[:, :, kper(-1)], E[:, :, kper(1)], E[:, :, kper(2)], rp)[I, J, :]
+        G1 = asg * (b(gu[0, 0]) * v[1] + b(gu[0, 2]) * v[3])
+        H = b(self.alpha * self.sqrtg * gu[1, 1]) * v[2]
+        H[:, :3] = -H[:, :3]           # the flux takes the sign of sin(theta) on the ghost rows
+        H[:, NJ - 3:] = -H[:, NJ - 3:]
+        Fp = asg * (b(gu[0, 2]) * v[1] + b(gu[2, 2]) * v[3])
+        t1 = self.cdiv(self.d4r(G1, rr), sg)[I, J, K]
+        t2 = self.cdiv(self.d4c(H[:, jsh(-2)], H[:, jsh(-1)], H[:, jsh(1)], H[:, jsh(2)], rt), sg[:, J])[I, :, K]
+        t3 = self.cdiv(self.d4c(Fp[:, :, kper(-2)], Fp[:, :, kper(-1)], Fp[:, :, kper(1)], Fp[:, :, kper(2)], rp),
+                       sg)[I, J, :]
+        t4 = (v[4] * dxb)[I, J, K]
+        t5 = self.cdiv(b1 * self.d4r(v[4] * sg, rr), sg)[I, J, K]
+        t6 = (b(self.alpha * (self.m * self.m)) * v[0])[I, J, K]
+        r[4] = t1 + t2 + t3 + t4 + t5 - t6
+        for w in range(5):
+            u = v[w]
+            a = r[w].copy()
+            kor = slice(3, n - 2)        # r planes 3 .. n-3 take the r dissipation
+            a[kor] = a[kor] + kr * self.ko6(*(u[3 + d:n - 2 + d, J, K] for d in (-3, -2, -1, 0, 1, 2, 3)))
+            a = a + kt * self.ko6(*(u[I, jsh(d), K] for d in (-3, -2, -1, 0, 1, 2, 3)))
+            a = a + kp * self.ko6(*(u[I, J][:, :, kper(d)] if d else u[I, J, K] for d in (-3, -2, -1, 0, 1, 2, 3)))
+            out[w, I, J, K] = a
+        return out
+
+    def boundary_cfg(self):
+        u, nz = self.u, self.Nz
+        u[:, :, :, 0] = u[:, :, :, nz - 1]
+        u[:, :, :, nz] = u[:, :, :, 1]
+        dis = nz // 2
+        sgn = np.array([1.0, 1.0, -1.0, 1.0, 1.0])[:, None]
+        for k in range(0, nz + 1):
+            kt = (k + dis) % (nz - 1)
+            for gg in range(self.g, -1, -1):
+                u[:, :, -gg - self.jL, k] = sgn * u[:, :, gg + 1 - self.jL, kt]
+                u[:, :, self.Ny + gg - self.jL, k] = sgn * u[:, :, self.Ny - gg - 1 - self.jL, kt]
+
+    def rk4_cfg(self):
+        dt = self.dt
+        up = self.u.copy()
+        ks = []
+        for rk in (1, 2, 3, 4):
+            kk = self.rhs_cfg(self.u) * dt
+            ks.append(kk)
+            if rk in (1, 2):
+                self.u = up + 0.50 * kk
+            elif rk == 3:
+                self.u = up + kk
+            else:
+                self.u = up + self.cdiv(ks[0] + 2.0 * ks[1] + 2.0 * ks[2] + ks[3], 6.0)
+            self.boundary_cfg()
+        self.t += dt
+
     # ---- Fortran-order state helpers: u(5, NI, NJ, NK) complex, var fastest
     def set_state(self, fortran_u):
         self.u = np.ascontiguousarray(np.asarray(fortran_u).reshape(self.NK, self.NJ, self.NI, 5).transpose(3, 2, 1, 0))
