@@ -407,6 +407,43 @@ class NumpyKG:
             self.boundary_cfg()
         self.t += dt
 
+    # ---- diagnostics (MoL/diagnostic_lib.f90:277-289, tools/integral.f90:220-255, 646-674)
+    def density(self):
+        """rho = 1/2 (|Pi| + g^rr |psi1|^2 + 2 g^rphi |psi1| psi3 + g^thth |psi2|^2
+        + g^phph |psi3|^2 + m^2 |phi|), real part, in the reference's term order"""
+        b, gu, u = self._b, self.gamma_up, self.u
+        # |z| as the Fortran abs of a complex value (cabs = hypot); numpy's
+        # complex abs uses its own algorithm and differs in the last bit
+        a1, a2, a3, a4, a5 = (np.hypot(u[w].real, u[w].imag) for w in range(5))
+        re = a5 + b(gu[0, 0]) * (a2 * a2)
+        re = re + (2.0 * b(gu[0, 2]) * a2) * u[3].real
+        re = re + b(gu[1, 1]) * (a3 * a3)
+        re = re + b(gu[2, 2]) * (a4 * a4)
+        re = re + (self.m * self.m) * a1
+        return 0.5 * re
+
+    def integrate_real(self, f):
+        """nested trapezium over i in 0..Nx, j in 0..Ny, all k: phi first, then
+        theta, then r, each sum accumulated in index order"""
+        g = self.g
+        f = f[g:g + self.Nx + 1, g:g + self.Ny + 1, :]
+        f2 = np.zeros(f.shape[:2])
+        for k in range(f.shape[2] - 1):
+            f2 = f2 + f[:, :, k] + f[:, :, k + 1]
+        f2 = 0.50 * f2 * self.dz
+        f1 = np.zeros(f.shape[0])
+        for j in range(f.shape[1] - 1):
+            f1 = f1 + f2[:, j] + f2[:, j + 1]
+        f1 = 0.50 * f1 * self.dy
+        f0 = 0.0
+        for i in range(f.shape[0] - 1):
+            f0 = f0 + f1[i] + f1[i + 1]
+        return 0.50 * f0 * self.dx
+
+    def mass(self):
+        """Mass_scalar = integrate(rho sqrt(gamma))"""
+        return self.integrate_real(self.density() * self._b(self.sqrtg))
+
     # ---- Fortran-order state helpers: u(5, NI, NJ, NK) complex, var fastest
     def set_state(self, fortran_u):
         self.u = np.ascontiguousarray(np.asarray(fortran_u).reshape(self.NK, self.NJ, self.NI, 5).transpose(3, 2, 1, 0))
