@@ -34,6 +34,7 @@ class NumpyKG:
         dxr = (xmax - xmin) / 1.0
         self.xmin = xmin + 0.0 * dxr
         self.xmax = xmin + 1.0 * dxr
+        self.xmax_param = xmax
         self.dx = (self.xmax - self.xmin) / float(Nx)
         self.dy = pi / float(Ny - 1)
         self.dz = 2.0 * pi / float(Nz - 1)
@@ -443,6 +444,144 @@ class NumpyKG:
     def mass(self):
         """Mass_scalar = integrate(rho sqrt(gamma))"""
         return self.integrate_real(self.density() * self._b(self.sqrtg))
+
+    # ---- detectors and their diagnostics (MoL/diagnostic_lib.f90:124-134, 219-274,
+    # main/global_numbers.f90:152-164, tools/FFT_sph.f90:247-279, 525-651,
+    # tools/integral.f90:330-362); complex products are written out component by
+    # component, as the Fortran compiler emits them
+    def detectors(self, n_det):
+        r = np.zeros(n_det)
+        idx = np.zeros(n_det, int)
+        r[0] = 1.0 + math.sqrt(1.0 - self.a * self.a)
+        r[-1] = self.xmax_param * 0.99
+        for d in range(2, n_det):
+            r[d - 1] = r[0] + (r[-1] - r[0]) / float(n_det) * float(d - 1)
+        for d in range(n_det):
+            for i in range(1, self.Nx):
+                if self.xmin + float(i - 1) * self.dx <= r[d] <= self.xmin + float(i) * self.dx:
+                    idx[d] = i
+                    break
+        return r, idx
+
+    def _active(self, r, idx):
+        return self.xmin <= r < self.xmin + float(self.Nx - 1) * self.dx and idx > 0
+
+    def domain_to_sph_shell(self, f, iv):
+        """f (NI, NJ, NK) complex on the evolution grid -> its values on the vertex
+        sphere of radius xmin + (iv - 1) dx, (Ny, Nz) [theta, phi]: index search
+        in each direction, then trilinear interpolation (phi, theta, r); the
+        theta rows outside the cell-centred grid copy the edge row"""
+        iL, iR, jL, jR, kL, kR = self.iL, self.iR, self.jL, self.jR, self.kL, self.kR
+        RD = lambda i: self.x[i - iL]
+        TD = lambda j: self.y[j - jL]
+        PD = lambda k: float(k) * self.dz
+        rmin, dr = RD(iL), RD(iL + 1) - RD(iL)
+        thetamin, dth = TD(jL), abs(TD(jL + 1) - TD(jL))
+        phimin, dph = PD(kL), abs(PD(kL + 1) - PD(kL))
+
+        def search(v, vmin, d, lo, hi, at):
+            i = int((v - vmin) / d) + lo
+            i = max(lo, min(i, hi - 1))
+            while i < hi - 1 and v >= at(i + 1):
+                i += 1
+            while i > lo and v < at(i):
+                i -= 1
+            return i
+
+        rr = self.xmin + float(iv - 1) * self.dx
+        ir = search(rr, rmin, dr, iL, iR, RD)
+        out = np.zeros((self.Ny, self.Nz), np.complex128)
+        for kv in range(1, self.Nz + 1):
+            pp = float(kv - 1) * self.dz
+            ip = search(pp, phimin, dph, kL, kR, PD)
+            for jv in range(1, self.Ny + 1):
+                tt = float(jv - 1) * self.dy
+                it = search(tt, thetamin, dth, jL, jR, TD)
+                if tt <= thetamin:
+                    out[jv - 1, kv - 1] = f[ir - iL, 0, ip]
+                    continue
+                if tt >= thetamin + dth * float(jR - jL):
+                    out[jv - 1, kv - 1] = f[ir - iL, jR - jL, ip]
+                    continue
+                wr, wt, wp = (rr - RD(ir)) / dr, (tt - TD(it)) / dth, (pp - PD(ip)) / dph
+                c = lambda di, dj, dk: f[ir - iL + di, it - jL + dj, ip + dk]
+
+                def lin(w, a, b):
+                    return complex((1.0 - w) * a.real + w * b.real, (1.0 - w) * a.imag + w * b.imag)
+                f00, f01 = lin(wp, c(0, 0, 0), c(0, 0, 1)), lin(wp, c(0, 1, 0), c(0, 1, 1))
+                f10, f11 = lin(wp, c(1, 0, 0), c(1, 0, 1)), lin(wp, c(1, 1, 0), c(1, 1, 1))
+                out[jv - 1, kv - 1] = lin(wr, lin(wt, f00, f01), lin(wt, f10, f11))
+        return out
+
+    def _trap_weights(self, j, k):
+        sel = (1 if j in (1, self.Ny) else 0) + 2 * (1 if k in (1, self.Nz) else 0)
+        return None if sel == 0 else (0.25 if sel == 3 else 0.5)
+
+    def project_sh(self, sl, Y, L):
+        """a_lm (2L+1, L+1) [m+L, l] of a sphere slice (Ny, Nz) against the Y_lm table
+        Y (Nz, Ny, 2L+1, L+1): trapezium of f conj(Y) sin(theta), summed in index order"""
+        ire = np.zeros((2 * L + 1, L + 1))
+        iim = np.zeros_like(ire)
+        for j in range(1, self.Ny + 1):
+            st = math.sin(float(j - 1) * self.dy)
+            for k in range(1, self.Nz + 1):
+                a = sl[j - 1, k - 1]
+                y = Y[k - 1, j - 1]
+                cre, cim = y.real, -y.imag
+                fre = (a.real * cre - a.imag * cim) * st
+                fim = (a.real * cim + a.imag * cre) * st
+                w = self._trap_weights(j, k)
+                if w is None:
+                    ire, iim = ire + fre, iim + fim
+                else:
+                    ire, iim = ire + w * fre, iim + w * fim
+        wq = self.dy * self.dz
+        out = np.empty(ire.shape, np.complex128)
+        out.real, out.imag = wq * ire, wq * iim
+        return out
+
+    def trap2d(self, sl):
+        re = im = 0.0
+        for j in range(1, self.Ny + 1):
+            for k in range(1, self.Nz + 1):
+                v = sl[j - 1, k - 1]
+                w = self._trap_weights(j, k)
+                if w is None:
+                    re, im = re + v.real, im + v.imag
+                else:
+                    re, im = re + w * v.real, im + w * v.imag
+        wq = self.dy * self.dz
+        return complex(wq * re, wq * im)
+
+    def proyector_detectors(self, Y, L, n_det):
+        r, idx = self.detectors(n_det)
+        out = np.zeros((n_det, 2 * L + 1, L + 1), np.complex128)
+        for d in range(n_det):
+            if self._active(r[d], idx[d]):
+                out[d] = self.project_sh(self.domain_to_sph_shell(self.u[0], idx[d]), Y, L)
+        return out
+
+    def currents_detectors(self, n_det):
+        """momentum(3, n_det): trapezium over the detector sphere of sqrt(gamma) j_i,
+        j_i = -Pi gamma^ij psi_j (currents_ADM), real part"""
+        b, gu, u = self._b, self.gamma_up, self.u
+        n5r, n5i = -u[4].real, -u[4].imag
+
+        def cx(ar, ai):  # (-Pi) times (ar + i ai), component-wise
+            return n5r * ar - n5i * ai, n5r * ai + n5i * ar
+        a = b(gu[0, 0]) * u[1] + b(gu[0, 2]) * u[3]
+        bb = b(gu[1, 1]) * u[2]
+        c = b(gu[0, 2]) * u[1] + b(gu[2, 2]) * u[3]
+        r, idx = self.detectors(n_det)
+        out = np.zeros((n_det, 3))
+        for comp, z in enumerate((a, bb, c)):
+            jr, ji = cx(z.real, z.imag)
+            g = np.empty(jr.shape, np.complex128)
+            g.real, g.imag = jr * b(self.sqrtg), ji * b(self.sqrtg)
+            for d in range(n_det):
+                if self._active(r[d], idx[d]):
+                    out[d, comp] = self.trap2d(self.domain_to_sph_shell(g, idx[d])).real
+        return out
 
     # ---- Fortran-order state helpers: u(5, NI, NJ, NK) complex, var fastest
     def set_state(self, fortran_u):
