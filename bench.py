@@ -53,13 +53,17 @@ PIRK2_MIN_BYTES = 416  # fused minimum per point-step: read u, stale Pi, u_stage
 
 
 def workload_config(w):
+    full = (w["Nx"], w["Ny"], w["Nz"]) == (2048, 129, 257)
     return {
-        "workload": "FP64 PIRK2 large solve: Nx=2048 Ny=129 Nz=257 (Nr=2048, Ntheta=128, Nphi=256), "
-                    "r in [1.8,400], Kerr-Schild M=1, m=0.3, outflow, CFL 0.25 reference dt rule",
+        "workload": f"FP64 PIRK2 {'large solve' if full else 'reduced grid'}: Nx={w['Nx']} Ny={w['Ny']} "
+                    f"Nz={w['Nz']} (Nr={w['Nx']}, Ntheta={w['Ny'] - 1}, Nphi={w['Nz'] - 1}), "
+                    f"r in [{w['xmin']:g},{w['xmax']:g}], Kerr-Schild M=1, m={w['m']:g}, outflow, "
+                    f"CFL {w['CFL']:g} reference dt rule",
         "grid": [w["Nx"], w["Ny"], w["Nz"]],
         "stepper": "pirk2",
         "refinement": "none (single level)",
-        "l2": "inputs larger than L2 (5.7 GB per state copy)",
+        "l2": (("inputs larger than L2 (%.1f GB per state copy)" if 5 * 16 * stored_points(w) > 2 * 126e6 else
+                "reduced grid: %.2f GB per state copy, not flushed between steps") % (5 * 16 * stored_points(w) / 1e9)),
         "seed": w["seed"],
     }
 
@@ -136,23 +140,32 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(w, threads, nx_sample=128, steps=150):
-    """The oracle (CPU restatement of the reference path) on a radial slab of the
-    workload: same theta x phi grid, Nx = nx_sample cells, `steps` PIRK2 steps."""
+def oracle_on_workload(w, threads):
+    """The oracle (CPU restatement of the reference path) on the workload grid
+    itself, loaded with the same seeded initial data as the GPU arm."""
     from oracle.oracle import Oracle, set_threads
     from kg_b200.initial_data import shell_ylm
     set_threads(threads)
-    Nx = nx_sample
-    xmax = w["xmin"] + (w["xmax"] - w["xmin"]) * Nx / w["Nx"]
-    o = Oracle(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, CFL=w["CFL"], m=w["m"])
-    u0, _ = shell_ylm(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, seed=w["seed"], r0=8.0)
+    o = Oracle(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], CFL=w["CFL"], m=w["m"])
+    u0, _ = shell_ylm(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], seed=w["seed"])
     o.set_state(u0)
-    o.pirk2(1)  # warm
+    del u0
+    return o
+
+
+def cpu_baseline(w, threads, steps=3):
+    """A bounded sample of the same workload on the host cores: `steps` PIRK2
+    steps of the oracle on the full workload grid (after one untimed step that
+    pages its arrays in)."""
+    o = oracle_on_workload(w, threads)
+    o.pirk2(1)
     t0 = time.perf_counter()
     o.pirk2(steps)
     dt = time.perf_counter() - t0
-    gpsu = Nx * (w["Ny"] - 1) * (w["Nz"] - 1) * 2 * steps / dt
-    return gpsu, dt, f"PIRK2 x{steps} on the Nx={Nx} radial slab of the workload grid ({Nx}x{w['Ny']}x{w['Nz']})"
+    o.close()
+    gpsu = interior_points(w) * 2 * steps / dt
+    return gpsu, dt, (f"PIRK2 x{steps} on the full workload grid ({w['Nx']}x{w['Ny']}x{w['Nz']}), "
+                      f"after one untimed step")
 
 
 SERVE_DESC = ("scaled serving workload: Poisson arrivals at 2000/s (the offered load exceeds one GPU's "
@@ -518,37 +531,86 @@ def projection_leg(mol, lib, h, L=64, reps=3):
 
 
 def run_reference(args):
-    from kg_b200 import replicas
+    """The reference arm: the CPU restatement of the reference's PIRK2 path
+    (the oracle; the Fortran/MPI reference cannot be built on this image) on
+    the same workload grid, initial data, metric and unit as the GPU arm, all
+    host threads, one PIRK2 step per step.  Only the oracle's library is
+    mapped: the package's solver library stays unloaded."""
+    from kg_b200 import capi, replicas
     _, rank, _ = replicas.rank_env()
     if rank != 0:
         return 0
     w = WORKLOAD
     threads = os.cpu_count() or 1
-    from oracle.oracle import Oracle, set_threads
-    from kg_b200.initial_data import shell_ylm
-    set_threads(threads)
-    Nx = 128
-    xmax = w["xmin"] + (w["xmax"] - w["xmin"]) * Nx / w["Nx"]
-    o = Oracle(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, CFL=w["CFL"], m=w["m"])
-    u0, _ = shell_ylm(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, seed=w["seed"], r0=8.0)
-    o.set_state(u0)
+    o = oracle_on_workload(w, threads)
     for _ in range(args.warmup):
         o.pirk2(1)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         o.pirk2(1)
     el = time.perf_counter() - t0
-    pts = Nx * (w["Ny"] - 1) * (w["Nz"] - 1)
-    val = pts * 2 * args.steps / el
-    sample = f"PIRK2 on the Nx={Nx} radial slab of the workload grid ({Nx}x{w['Ny']}x{w['Nz']}), one step per step"
+    o.close()
+    if capi._lib is not None:
+        raise RuntimeError("the reference arm mapped libkg_b200.so")
+    val = interior_points(w) * 2 * args.steps / el
+    sample = (f"PIRK2 on the full workload grid ({w['Nx']}x{w['Ny']}x{w['Nz']}), one step per step, "
+              f"{args.warmup} untimed warm-up steps")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-            "data": "synthetic (seeded)", "config": workload_config(w),
+            "data": "synthetic (seeded Gaussian shell x Y_lm, l<=4)",
+            "config": dict(workload_config(w), parallelism="host threads"),
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def summarize(line, steps):
+    """The numbers of every leg in one short object (kept as the line's last key)."""
+    g = lambda d, *ks: _dig(d, ks)
+    out = {"pirk2_ggpsu": line["value"] / 1e9, "ms_per_step": line["ms_per_step"],
+           "roofline_frac": g(line, "roofline", "frac"), "step_hbm_frac": line["step_bandwidth_gbs"] /
+           line["roofline"]["peak"] if line.get("roofline") else None,
+           "e2e_ggpsu": (line["e2e"]["value"] / 1e9) if line.get("e2e") else None, "e2e_steps": steps,
+           "steppers_ggpsu": {k: v / 1e9 for k, v in line.get("steppers_gpsu", {}).items()},
+           "cpu_baseline_mgpsu": (g(line, "cpu_baseline", "value") or 0) / 1e6 or None}
+    if "projection" in line:
+        p = line["projection"]
+        out["projection"] = {"gemm_ms": p["gemm_ms"], "tensor_frac": g(p, "tensor_roofline", "frac"),
+                             "energy_rel_err": p["energy_norm_rel_err_vs_fp64"]}
+    if "precision" in line:
+        p = line["precision"]
+        out["precision"] = {"step_speedup": p["step_speedup"], "combined_speedup": p["combined_speedup"],
+                            "phi_rel_err": p["phi_rel_l2_err"], "pi_rel_err": p["pi_rel_l2_err"],
+                            "wave_r12_rel_err": g(p, "waveform_r12", "rel_l2"),
+                            "wave_r50_rel_err": g(p, "waveform_r50", "rel_l2"), "steps": p.get("steps")}
+    if "refinement" in line:
+        r = line["refinement"]
+        out["refinement_ggpsu"] = {k: r[k]["gpsu"] / 1e9 for k in ("rk4", "rk3", "pirk2") if k in r}
+        if "waveform_r50" in r:
+            out["refinement_wave_r50_rel_err"] = g(r, "waveform_r50", "rel_l2")
+    if "c0_configured" in line:
+        out["c0_ms_per_step"] = line["c0_configured"]["ms_per_step"]
+    if "batching" in line:
+        e = line["batching"]["engine_device_time"]
+        out["batching_speedup"] = {"fp64": e["speedup_batched_fp64"], "mixed": e["speedup_batched_mixed"]}
+    if "serving" in line:
+        sv = line["serving"]
+        out["serving"] = {"solves_per_s": {k: g(sv, k, "solves_per_s") for k in
+                                           ("plain_fp64", "batched_fp64", "batched_mixed")},
+                          "speedup_mixed": sv["speedup_batched_mixed"],
+                          "device_speedup_mixed": g(sv, "engine_device_time", "speedup_batched_mixed"),
+                          "wave_err_mixed": g(sv, "waveform_batched_mixed_vs_plain_fp64", "max_rel_l2")}
+    return out
+
+
+def _dig(d, ks):
+    for k in ks:
+        if not isinstance(d, dict) or k not in d:
+            return None
+        d = d[k]
+    return d
 
 
 def main():
@@ -667,6 +729,7 @@ def main():
     f1.record(stream)
     f1.synchronize()
     e2e_ms = replicas.max_over_ranks(f0.elapsed_time(f1), world, device=f"cuda:{local}")
+    del host_u0, host_out, p_in, p_out  # 11 GB of pinned host memory, not needed by the legs below
 
     pts = interior_points(w)
     value = replicas.job_rate(pts * 2 * args.steps, world, el_ms)
@@ -718,6 +781,7 @@ def main():
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
                                 "seconds": secs}
     if rank == 0:
+        line["summary"] = summarize(line, args.steps)  # last key: the side legs in a few numbers
         print(json.dumps(line), flush=True)
     mol.close()
     replicas.finish(world)

@@ -179,7 +179,11 @@ int kg_set_detectors(kg_solver *h, int n, const double *radii);
  * u(1:5,-g:Nx+g,-g:Ny+g,0:Nz).  The stage arrays carry the previous step's Pi
  * that PIRK stage 1 reads, so loading into a handle of the same grid resumes
  * bit for bit (the reference's text checkpoint keeps u and t only, and its
- * reader deletes the file before opening it). */
+ * reader deletes the file before opening it).  Load returns KG_EINVAL, with the
+ * handle unchanged, when the file's grid, metric, outer BC, field mass, xmin,
+ * xmax, scheme (and Kreiss-Oliger eps) or precision mode differ from the
+ * handle's, or when the file is truncated; stage arrays the file lacks are
+ * reset to a fresh handle's (zero, Pi slot 4). */
 int kg_save_checkpoint(kg_solver *h, const char *path);
 int kg_load_checkpoint(kg_solver *h, const char *path);
 /* detector radii and vertex indices (1-based) */

@@ -4,13 +4,13 @@ FlavioRosales/KG Fortran code.
 
 The solver lives in libkg_b200.so behind the C ABI of include/kg_capi.h;
 `LinesMethod` / `ScalarField` mirror the reference's Fortran objects on top of
-it.  Importing the package loads the library and fails loudly if it has not
-been built.
+it.  The library is mapped on first use (`capi.load()`, called by every solver
+constructor), so host-only modules of the package (request drawing, replica
+plumbing, initial data) import without it; any solver operation fails loudly
+with an ImportError if it has not been built.
 """
 from . import capi
 from .capi import KgError, KgParams
 from .lines_method import LinesMethod, ScalarField
-
-capi.load()
 
 __all__ = ["capi", "KgError", "KgParams", "LinesMethod", "ScalarField"]

@@ -1757,34 +1757,67 @@ int kg_load_checkpoint(kg_solver* h, const char* path) {
   FILE* f = fopen(path, "rb");
   if (!f) return set_err(h, KG_EINVAL, std::string("cannot open for reading: ") + path);
   CkptHeader hd;
-  int rc = KG_OK;
   if (fread(&hd, sizeof(hd), 1, f) != 1 || memcmp(hd.magic, "KGB2CKPT", 8) != 0 || hd.version != 1) {
     fclose(f);
     return set_err(h, KG_EINVAL, "not a checkpoint of this library");
   }
-  if (hd.Nx != h->Nx || hd.Ny != h->Ny || hd.Nz != h->Nz || hd.g_pts != h->p.g_pts) {
+  // the state only means the same thing on the same grid, metric, outer
+  // boundary, field mass, radial extent and method
+  std::string why;
+  if (hd.Nx != h->Nx || hd.Ny != h->Ny || hd.Nz != h->Nz || hd.g_pts != h->p.g_pts)
+    why = "checkpoint grid differs from the handle's grid";
+  else if (hd.metric != h->p.metric)
+    why = "checkpoint metric differs from the handle's metric";
+  else if (hd.bc_rmax != h->p.bc_rmax)
+    why = "checkpoint outer boundary condition differs from the handle's";
+  else if (hd.m != h->p.m)
+    why = "checkpoint field mass differs from the handle's";
+  else if (hd.xmin != h->p.xmin || hd.xmax != h->p.xmax)
+    why = "checkpoint radial extent (xmin, xmax) differs from the handle's";
+  else if (hd.scheme != h->scheme || (hd.scheme == 1 && hd.ko_eps != h->ko_eps))
+    why = "checkpoint method (scheme, Kreiss-Oliger eps) differs from the handle's; call kg_set_scheme first";
+  else if (hd.precision != h->precision)
+    why = "checkpoint precision mode differs from the handle's; call kg_set_precision first";
+  else if (hd.has_stage < 0 || hd.has_stage > 1 || hd.has_stage2 < 0 || hd.has_stage2 > 1)
+    why = "checkpoint header is corrupt";
+  if (!why.empty()) {
     fclose(f);
-    return set_err(h, KG_EINVAL, "checkpoint grid differs from the handle's grid");
+    return set_err(h, KG_EINVAL, why);
   }
+  // read the whole file before touching the handle, so a truncated or
+  // unreadable file leaves it as it was
   const size_t n = (size_t)5 * h->NI * h->NJ * h->NK * 2;
+  const int have[3] = {1, hd.has_stage, hd.has_stage2};
+  const int nstates = have[0] + have[1] + have[2];
   std::vector<double> buf;
   try {
-    buf.resize(n);
+    buf.resize(n * nstates);
   } catch (...) {
     fclose(f);
     return set_err(h, KG_ENOMEM, "host buffer for the checkpoint");
   }
-  const int have[3] = {1, hd.has_stage, hd.has_stage2};
-  for (int w = 0; w < 3 && rc == KG_OK; ++w) {
-    if (!have[w]) continue;
-    if (fread(buf.data(), sizeof(double), n, f) != n) {
-      rc = set_err(h, KG_EINVAL, "checkpoint truncated");
-      break;
-    }
-    rc = kg_set_state(h, w, buf.data());
-  }
+  const bool complete = fread(buf.data(), sizeof(double), n * nstates, f) == n * nstates;
   fclose(f);
-  if (rc) return rc;
+  if (!complete) return set_err(h, KG_EINVAL, "checkpoint truncated");
+  int rc;
+  size_t at = 0;
+  for (int w = 0; w < 3; ++w) {
+    if (!have[w]) continue;
+    if ((rc = kg_set_state(h, w, buf.data() + at))) return rc;
+    at += n;
+  }
+  // stage arrays the file does not hold return to the state of a fresh
+  // handle: zero, with the current Pi value in slot 4 (PIRK stage 1 reads it
+  // as the previous step's Pi)
+  if (!hd.has_stage) {
+    h->s_cur = 4;
+    if (h->S) KG_CK(cudaMemsetAsync(h->S, 0, 6 * field_bytes(h), h->stream));
+  }
+  if (!hd.has_stage2) {
+    h->t_cur = 4;
+    if (h->T) KG_CK(cudaMemsetAsync(h->T, 0, 6 * field_bytes(h), h->stream));
+  }
+  KG_CK(cudaStreamSynchronize(h->stream));
   h->t = hd.t;
   h->dt = hd.dt;
   return KG_OK;

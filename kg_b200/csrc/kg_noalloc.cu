@@ -46,12 +46,14 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_scratch_ptr[kMaxDevices] = {};
 
-// f2d(a, b) = 0.5 dz sum_k (f(k) + f(k+1)),  f = rho * sqrtg at i = a, j = b
+// f2d(a, b) = 0.5 dz sum_k (f(k) + f(k+1)),  f = rho * sqrtg at i = a, j = b;
+// one thread per (a, b) column on a 1-D grid (a fastest, so loads coalesce along r)
 __global__ void noalloc_phi_sum(const double* __restrict__ rho, const double* __restrict__ sqrtg, int Nx, int Ny,
                                 int Nz, double dz, double* __restrict__ f2d) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = blockIdx.y;
-  if (a > Nx || b > Ny) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)(Nx + 1) * (Ny + 1)) return;
+  const int a = (int)(t % (Nx + 1));
+  const int b = (int)(t / (Nx + 1));
   const int NI = Nx + 5, NJ = Ny + 5;
   const int ii = a + 2, jj = b + 2;
   const double sg = sqrtg[(size_t)jj * NI + ii];
@@ -100,6 +102,7 @@ const char* kg_noalloc_last_error() { return t_err.c_str(); }
 
 extern "C" int kg_integrate_mass_noalloc(const double* rho_dev, const double* sqrtg_dev, int Nx, int Ny, int Nz,
                                          double dx, double dy, double dz, double* out_dev, void* stream) {
+  t_err.clear();  // kg_last_error(NULL) reports this call only
   if (!rho_dev || !sqrtg_dev || !out_dev || Nx < 1 || Ny < 1 || Nz < 1) {
     t_err = "kg_integrate_mass_noalloc: null pointer or non-positive grid size";
     return KG_EINVAL;
@@ -134,7 +137,8 @@ extern "C" int kg_integrate_mass_noalloc(const double* rho_dev, const double* sq
   cudaStream_t st = (cudaStream_t)stream;
   double* f2d = scratch;
   double* f1d = scratch + (size_t)(Nx + 1) * (Ny + 1);
-  noalloc_phi_sum<<<dim3((Nx + 1 + 127) / 128, Ny + 1), 128, 0, st>>>(rho_dev, sqrtg_dev, Nx, Ny, Nz, dz, f2d);
+  const unsigned cols_blocks = (unsigned)(((size_t)(Nx + 1) * (size_t)(Ny + 1) + 127) / 128);  // <= 4096
+  noalloc_phi_sum<<<cols_blocks, 128, 0, st>>>(rho_dev, sqrtg_dev, Nx, Ny, Nz, dz, f2d);
   noalloc_theta_sum<<<(Nx + 1 + 127) / 128, 128, 0, st>>>(f2d, Nx, Ny, dy, f1d);
   noalloc_r_sum<<<1, 32, 0, st>>>(f1d, Nx, dx, out_dev);
   e = cudaGetLastError();

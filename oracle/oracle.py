@@ -106,10 +106,13 @@ class Oracle:
         self.npts = self.NI * self.NJ * self.NK
         self.n_det = max(2, n_det)
 
-    def __del__(self):
+    def close(self):
         if getattr(self, "h", None):
             lib().kgo_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        self.close()
 
     # state in Fortran order: complex128, shape (NK, NJ, NI, 5) in C order
     def shape(self):

@@ -74,3 +74,27 @@ def test_mass_noalloc_rejects_oversized_grid():
     rc = lib.kg_integrate_mass_noalloc(p, p, 4096, 200, 8, 1.0, 1.0, 1.0, p, None)
     assert rc == capi.KG_EINVAL
     assert b"static scratch holds" in lib.kg_last_error(None)
+
+
+def test_mass_noalloc_wide_theta_grid_and_error_cleared():
+    """A grid with more theta rows than a launch's y-dimension allows (Ny + 1 >
+    65535) is within the scratch limit and runs; a successful call after a
+    rejected one leaves kg_last_error(NULL) empty."""
+    import torch
+    from kg_b200 import capi
+    lib = capi.load()
+    bad = torch.zeros(8, dtype=torch.float64, device="cuda")
+    pb = C.c_void_p(bad.data_ptr())
+    assert lib.kg_integrate_mass_noalloc(pb, pb, 4096, 200, 8, 1.0, 1.0, 1.0, pb, None) == capi.KG_EINVAL
+    Nx, Ny, Nz = 1, 100000, 1
+    NI, NJ = Nx + 5, Ny + 5
+    rho = torch.ones((Nz + 1) * NJ * NI, dtype=torch.float64, device="cuda")
+    sqrtg = torch.ones(NJ * NI, dtype=torch.float64, device="cuda")
+    out = torch.full((1,), np.nan, dtype=torch.float64, device="cuda")
+    rc = lib.kg_integrate_mass_noalloc(C.c_void_p(rho.data_ptr()), C.c_void_p(sqrtg.data_ptr()), Nx, Ny, Nz,
+                                       1.0, 1.0, 1.0, C.c_void_p(out.data_ptr()), None)
+    assert rc == capi.KG_OK, lib.kg_last_error(None)
+    torch.cuda.synchronize()
+    assert lib.kg_last_error(None) == b""
+    # trapezium of a constant 1 over [0, Nz] x [0, Ny] x [0, Nx] with unit spacings
+    assert float(out.item()) == float(Nx * Ny * Nz)
