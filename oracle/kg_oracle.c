@@ -1143,6 +1143,68 @@ void kgo_project_all_shells(const kgo *s, int L, double *alm) {
   free(sl); free(ylm);
 }
 
+/* project_all_shells restricted to the vertex shells listed in iv[0..n-1]
+ * (1-based), for spheres where the full Y_lm table does not fit: the same
+ * Y_lm values (sph_harmonics' formulas) and the same trapezium order as
+ * kgo_project_sh, so every coefficient equals kgo_project_all_shells' bit for
+ * bit; Y_lm is formed per (l, m) on the fly instead of from a stored table.
+ * out: n x (2L+1) x (L+1) complex, l fastest.  Threads over (l, m). */
+void kgo_project_shells(const kgo *s, int L, int n, const int *iv, double *alm) {
+  const int NL = L + 1, NM = 2 * L + 1, Nth = s->Ny, Nph = s->Nz;
+  const size_t per = (size_t)NL * NM, sz = (size_t)Nth * Nph;
+  const double pi = acos(-1.0);
+  cplx *F = (cplx *)alm;
+  memset(F, 0, sizeof(cplx) * per * (size_t)n);
+  cplx *sl = xcalloc(sz * (size_t)n, sizeof(cplx));
+  for (int q = 0; q < n; ++q) kgo_domain_to_sph_shell(s, s->u[0], iv[q], sl + sz * (size_t)q);
+  double *st = xcalloc(Nth, sizeof(double));
+  for (int j = 1; j <= Nth; ++j) st[j - 1] = sin((double)(j - 1) * s->dy);
+  #pragma omp parallel for schedule(dynamic, 1)
+  for (int lm = 0; lm < NL * NL; ++lm) {
+    const int l = lm / NL, m = lm % NL;
+    if (m > l) continue;
+    double fact = sqrt((2.0 * l + 1.0) / (4.0 * pi));
+    double norm = fact;
+    if (m > 0) for (int i = 1; i <= 2 * m; ++i) norm = norm / sqrt((double)(l - m + i));
+    cplx *Y = malloc(sizeof(cplx) * sz);
+    if (!Y) abort();
+    for (int jv = 1; jv <= Nth; ++jv) {
+      double x = cos((double)(jv - 1) * s->dy), P;
+      if (fabs(x) > 0.9999) P = (m == 0) ? fact : 0.0;
+      else P = plm(l, m, x);
+      for (int kv = 1; kv <= Nph; ++kv) {
+        double ph = (double)(kv - 1) * s->dz;
+        cplx phase = {cos(m * ph), sin(m * ph)};
+        Y[(jv - 1) + (size_t)Nth * (kv - 1)] = rmul(norm * P, phase);
+      }
+    }
+    for (int sgn = 0; sgn < (m > 0 ? 2 : 1); ++sgn) {
+      const int mm = sgn ? -m : m;
+      const double sg = (m % 2) ? -1.0 : 1.0;
+      for (int q = 0; q < n; ++q) {
+        const cplx *f = sl + sz * (size_t)q;
+        cplx integ = {0.0, 0.0};
+        for (int j = 1; j <= Nth; ++j)
+          for (int k = 1; k <= Nph; ++k) {
+            cplx a = f[(j - 1) + (size_t)Nth * (k - 1)];
+            cplx y = Y[(j - 1) + (size_t)Nth * (k - 1)];
+            if (sgn) y = (cplx){sg * y.re, sg * -y.im};
+            cplx c = {y.re, -y.im};
+            cplx fy = {a.re * c.re - a.im * c.im, a.re * c.im + a.im * c.re};
+            cplx fun = {fy.re * st[j - 1], fy.im * st[j - 1]};
+            int sel = ((j == 1 || j == Nth) ? 1 : 0) + 2 * ((k == 1 || k == Nph) ? 1 : 0);
+            if (sel == 0) integ = cadd(integ, fun);
+            else if (sel == 3) integ = cadd(integ, rmul(0.25, fun));
+            else integ = cadd(integ, rmul(0.5, fun));
+          }
+        F[per * (size_t)q + l + NL * (mm + L)] = rmul(s->dy * s->dz, integ);
+      }
+    }
+    free(Y);
+  }
+  free(st); free(sl);
+}
+
 /* spherical Bessel j_l(x) (GSL's gsl_sf_bessel_jl in the reference,
  * tools/FFT_sph.f90:29-34; GSL is not available here): Miller's downward
  * recurrence j_{k-1} = (2k+1)/x j_k - j_{k+1} from an order above both l and

@@ -66,6 +66,7 @@ def lib():
         L.kgo_currents_detectors.argtypes = [P, D]
         L.kgo_proyector_detectors.argtypes = [P, I, D]
         L.kgo_project_all_shells.argtypes = [P, I, D]
+        L.kgo_project_shells.argtypes = [P, I, I, C.POINTER(C.c_int), D]
         L.kgo_set_scheme.argtypes = [P, I, C.c_double]
         L.kgo_set_scheme.restype = I
         L.kgo_boundary_cfg.argtypes = [P]
@@ -219,6 +220,15 @@ class Oracle:
         """a_lm on every vertex shell: (Nx, 2L+1, L+1) complex"""
         out = np.zeros((self.Nx, 2 * L + 1, L + 1), np.complex128)
         lib().kgo_project_all_shells(self.h, L, _dp(out.view(np.float64)))
+        return out
+
+    def project_shells(self, L, shells):
+        """a_lm on the listed vertex shells (1-based), equal to the same rows of
+        project_all_shells; for large spheres (no stored Y_lm table, threaded)"""
+        iv = np.ascontiguousarray(shells, dtype=np.int32)
+        out = np.zeros((len(iv), 2 * L + 1, L + 1), np.complex128)
+        lib().kgo_project_shells(self.h, L, len(iv), iv.ctypes.data_as(C.POINTER(C.c_int)),
+                                 _dp(out.view(np.float64)))
         return out
 
     def set_scheme(self, scheme, ko_eps=0.02):

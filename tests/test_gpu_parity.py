@@ -202,6 +202,35 @@ def test_c0_1000_steps_pirk2():
     assert np.array_equal(a, b)
 
 
+# a radial slab of the benchmark grid: the same theta x phi grid (Ny = 129,
+# Nz = 257: 134 stored rows, 258 planes), the same dr (r in [1.8, 400] over
+# 2048 cells) and the same ragged last r tile (165 = 5 x 32 + 5, as 2053 =
+# 64 x 32 + 5), so the default kernels run with the tiling, phi chunking and
+# pole partner planes of the benchmarked solve
+C1_SLAB = dict(Nx=160, Ny=129, Nz=257, xmin=1.8, xmax=1.8 + 398.2 * 160 / 2048)
+
+
+@pytest.mark.parametrize("method", ["pirk2", "pirk3", "rk3", "rk4"])
+def test_benchmark_sphere_steppers_bitexact(method):
+    """Default kernels (variant 2) on the benchmark's theta x phi grid, 3 steps
+    of each stepper, bit-exact against the oracle (threaded)."""
+    from oracle.oracle import set_threads, max_threads
+    set_threads(max_threads())
+    g = C1_SLAB
+    dev, ora = _pair(grid=g, m=0.3)
+    from kg_b200.initial_data import shell_ylm
+    u0, _ = shell_ylm(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], seed=20240601, r0=12.0, sd=1.0)
+    dev.u = u0
+    ora.set_state(u0)
+    for _ in range(3):
+        getattr(dev, method)(nsteps=1) if method.startswith("rk") else getattr(dev, method)(1)
+        ora.step(method, 1)
+    a, b = dev.u, ora.get_state()
+    assert np.array_equal(a, b), f"{method} max diff {np.abs(a - b).max()}"
+    if method.startswith("pirk"):
+        assert np.array_equal(dev.u_stage, ora.get_stage())
+
+
 def test_diagnostics_match_oracle():
     dev, ora = _pair(m=0.3, l_max=6, n_det=5)
     u0 = _ic(seed=9)

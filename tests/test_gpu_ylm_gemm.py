@@ -109,6 +109,24 @@ def test_tensor_core_repeat_and_degree_change():
     _check_split_bound(a_t, a_o, _shell_norms(ora, ora.get_state(), c), "after 2 steps:")
 
 
+def test_tensor_core_l64_on_the_benchmark_sphere():
+    """The precision form's projection: l <= 64 on the 129 x 257 vertex sphere
+    of the benchmark grid (K = 33153 sphere points, 2145 modes m >= 0), checked
+    on a few shells against the oracle within the split-BF16 bound."""
+    from oracle.oracle import set_threads, max_threads
+    set_threads(max_threads())
+    c = dict(Nx=24, Ny=129, Nz=257, L=64, xmin=1.8, xmax=6.5, seed=14)
+    for noise in (0.0, 0.05):
+        dev, ora = _pair(c, noise)
+        a_t = dev.project_all_shells(c["L"], precision=1)
+        shells = [2, 12, 20]
+        a_o = ora.project_shells(c["L"], shells)
+        fn = _shell_norms(ora, _state(c, noise), c)
+        _check_split_bound(a_t[[iv - 1 for iv in shells]], a_o, fn[[iv - 1 for iv in shells]],
+                           f"L=64 129x257 noise {noise}:")
+        dev.close()
+
+
 def test_detector_shell_agrees_with_all_shells():
     """the all-shell FP64 projection at a detector's shell is the detector projection"""
     from kg_b200 import ScalarField

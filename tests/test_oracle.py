@@ -249,6 +249,19 @@ def test_all_shell_projection_contains_detector_projection():
             assert np.array_equal(a_det[d], a_all[iv - 1])
 
 
+def test_shell_subset_projection_equals_all_shells():
+    """project_shells (Y_lm formed per mode, threaded) gives the same bits as
+    the rows of project_all_shells (stored Y_lm table)"""
+    g = GRID
+    o = Oracle(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], m=0.3)
+    o.set_state(_ic())
+    a_all = o.project_all_shells(7)
+    shells = [1, 3, g["Nx"]]
+    a_sub = o.project_shells(7, shells)
+    for q, iv in enumerate(shells):
+        assert np.array_equal(a_sub[q], a_all[iv - 1])
+
+
 def test_spherical_bessel_against_scipy():
     """j_l (gsl_sf_bessel_jl in the reference, tools/FFT_sph.f90:29-34) against
     scipy, relative to the function's envelope (|j_l| below l, sqrt(j_l^2 + y_l^2) above)"""
