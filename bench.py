@@ -45,10 +45,11 @@ WORKLOAD = dict(Nx=2048, Ny=129, Nz=257, xmin=1.8, xmax=400.0, m=0.3, CFL=0.25, 
 METRIC = "RK point-updates/s (FP64 PIRK2, Nr=2048 x Ntheta=128 x Nphi=256)"
 UNIT = "GPSU/s"
 # algorithmic bytes per stored point of each PIRK2 kernel (complex128 = 16 B per variable)
-#   stage_pirk_s1_psi: read u (5 vars) + write u_stage(1:4)               = 80 + 64
-#   stage_pirk_s1_pi : read u_stage(1:4), stale u_stage(5), u(5); write u_stage(5) = 64 + 16 + 16 + 16
-#   stage_pirk2_s2   : read u_stage, u_p(=u); write u                     = 80 + 80 + 80
-ALG_BYTES = {"stage_pirk_s1_psi": 144, "stage_pirk_s1_pi": 112, "stage_pirk2_s2": 240}
+#   stage_pirk_s1_fused: read u (5 vars), stale u_stage(5); write u_stage(1:5) = 80 + 16 + 80
+#   stage_pirk_s1_psi  : read u (5 vars) + write u_stage(1:4)               = 80 + 64   (two-launch form)
+#   stage_pirk_s1_pi   : read u_stage(1:4), stale u_stage(5), u(5); write u_stage(5) = 64 + 16 + 16 + 16
+#   stage_pirk2_s2     : read u_stage, u_p(=u); write u                     = 80 + 80 + 80
+ALG_BYTES = {"stage_pirk_s1_fused": 176, "stage_pirk_s1_psi": 144, "stage_pirk_s1_pi": 112, "stage_pirk2_s2": 240}
 PIRK2_MIN_BYTES = 416  # fused minimum per point-step: read u, stale Pi, u_stage, u; write u_stage, u
 
 

@@ -285,6 +285,13 @@ int kg_hier_rk4(kg_hier *H, int coarse_steps);
 /* the same hierarchy stepped by SSP-RK3 (rk3, MoL/lines_method_lib.f90:211-269);
  * the stage inputs stand at t, t+dt and t+dt/2 for the buffer-plane times */
 int kg_hier_rk3(kg_hier *H, int coarse_steps);
+/* the same hierarchy stepped by PIRK2 / PIRK3 (pirk2, MoL/lines_method_lib.f90:271-332;
+ * pirk3, :334-408).  u_stage stands at t+dt and u_stage_2 (PIRK3) at t+dt/2, so
+ * their buffer planes take the parent's state at those times, Pi included; the
+ * stale-Pi slot that stage 1 reads then holds, on the buffer planes, the
+ * parent's Pi at the step's start. */
+int kg_hier_pirk2(kg_hier *H, int coarse_steps);
+int kg_hier_pirk3(kg_hier *H, int coarse_steps);
 int kg_hier_synchronize(kg_hier *H);
 
 /* --- allocation-free diagnostic --------------------------------------------- */

@@ -110,6 +110,8 @@ SIGNATURES = [
     ("kg_hier_level", _P, [_P, _I]),
     ("kg_hier_rk4", _I, [_P, _I]),
     ("kg_hier_rk3", _I, [_P, _I]),
+    ("kg_hier_pirk2", _I, [_P, _I]),
+    ("kg_hier_pirk3", _I, [_P, _I]),
     ("kg_hier_synchronize", _I, [_P]),
     ("kg_batch_get_tuning", _I, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("kg_batch_launch_count", C.c_longlong, [_P]),

@@ -64,7 +64,8 @@ struct kg_solver {
   double* rho = nullptr;
   double* partials = nullptr;            // mass partial sums + result
   int s_cur = 4, t_cur = 4;              // slot holding the current Pi stage value
-  int variant = 2;                       // 0: per-point, 1: 2.5-D marching, 2: TMA-pipelined marching
+  int variant = 2;                       // 0: per-point, 1: 2.5-D marching, 2..5: TMA-pipelined marching
+                                         // (2, 4, 5: PIRK stage 1 fused in one kernel; 3: two launches)
   int* derr = nullptr;                   // device flag: a bounded wait in a kernel ran out
   // CUDA graphs of two consecutive steps per stepper and Pi-slot state
   int use_graphs = 1;
@@ -202,13 +203,13 @@ double2* fld(double2* base, const Grid& g, int v) { return base + (long long)v *
 // kernel kinds reported by kg_profile_read: the 13 stage kinds, then these
 enum { PK_GHOST = 13, PK_FACE, PK_RHS, PK_CONVERT, PK_DENSITY, PK_MASS, PK_SHELL, PK_FLUX, PK_PROJECT,
        PK_YLM_PREP, PK_YLM_GEMM, PK_YLM_FP64, PK_RADIAL, PK_MX1, PK_MX2, PK_MX3, PK_MX4, PK_GHOST_F32, PK_PROLONG,
-       PK_RESTRICT, PK_COUNT };
+       PK_RESTRICT, PK_S1_FUSED, PK_COUNT };
 const char* const kPkNames[PK_COUNT] = {
     "stage_pirk_s1_psi", "stage_pirk_s1_pi", "stage_pirk2_s2", "stage_pirk3_s2_psi", "stage_pirk3_s2_pi",
     "stage_pirk3_s3", "stage_rk3_1", "stage_rk3_2", "stage_rk3_3", "stage_rk4_1", "stage_rk4_2", "stage_rk4_3",
     "stage_rk4_4", "ghost_fill", "boundary_face", "rhs", "layout_convert", "density", "mass_reduce",
     "shell_interp", "flux_reduce", "ylm_project", "ylm_all_prepare", "ylm_all_gemm_bf16x3", "ylm_all_fp64", "radial_ft", "mixed_rk4_1",
-    "mixed_rk4_2", "mixed_rk4_3", "mixed_rk4_4", "ghost_fill_f32", "bo_prolong", "bo_restrict"};
+    "mixed_rk4_2", "mixed_rk4_3", "mixed_rk4_4", "ghost_fill_f32", "bo_prolong", "bo_restrict", "stage_pirk_s1_fused"};
 
 cudaEvent_t take_event(kg_solver* h) {
   if (!h->pool.empty()) {
@@ -713,7 +714,7 @@ int store_view(kg_solver* h, const View& V, double* dst, cudaMemcpyKind kind) {
 void run_stage(kg_solver* h, int kind, const kg::StageLaunch& L) {
   Prof pf(h, kind, 1);
   const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
-  if (h->variant == 2 && kg::launch_stage_tma(kind, L, rsg, h->derr, h->stream) == 0) return;
+  if (h->variant >= 2 && kg::launch_stage_tma(kind, L, rsg, h->derr, h->stream) == 0) return;
   if (h->variant >= 1)
     kg::launch_stage_march(kind, L, rsg, h->stream);
   else
@@ -748,6 +749,30 @@ kg::StageLaunch base_launch(kg_solver* h) {
 void set_in(kg::StageLaunch& L, const Grid& g, double2* b0, double2* b4) {
   for (int v = 0; v < 4; ++v) L.in[v] = fld(b0, g, v);
   L.in[4] = b4;
+}
+
+// PIRK stage 1 (pirk2 :278-289, pirk3 :341-352): u_stage(1:4) from u, then
+// u_stage(5) from u_stage(1:4) and the previous step's Pi in Sold; one fused
+// kernel for the TMA forms 2, 4 and 5, two launches otherwise
+void run_pirk_s1(kg_solver* h, double2* Sold, double2* Snew) {
+  const Grid& g = h->g;
+  const int cfg = h->variant == 2 ? 0 : h->variant == 4 ? 1 : h->variant == 5 ? 2 : -1;
+  if (cfg >= 0) {
+    Prof pf(h, PK_S1_FUSED, 1);
+    const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
+    const int mk = h->p.metric == KG_SCHW_EF ? kg::MK_SCHW : kg::MK_KS;
+    if (kg::launch_pirk_s1_fused(cfg, g, metric_of(h), mk, h->U, Sold, h->S, Snew, rsg, h->derr, h->stream) == 0)
+      return;
+    pf.n = 0;
+  }
+  kg::StageLaunch L = base_launch(h);
+  set_in(L, g, h->U, fld(h->U, g, 4));
+  L.base = h->U;
+  L.out = h->S;
+  run_stage(h, kg::ST_P2_S1A, L);
+  set_in(L, g, h->S, Sold);
+  L.out4 = Snew;
+  run_stage(h, kg::ST_P2_S1B, L);
 }
 
 }  // namespace
@@ -910,14 +935,9 @@ int step_pirk2(kg_solver* h, int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
     double2* Sold = fld(h->S, g, h->s_cur);
     double2* Snew = fld(h->S, g, 9 - h->s_cur);
+    run_pirk_s1(h, Sold, Snew);
     kg::StageLaunch L = base_launch(h);
-    set_in(L, g, h->U, fld(h->U, g, 4));
     L.base = h->U;
-    L.out = h->S;
-    run_stage(h, kg::ST_P2_S1A, L);
-    set_in(L, g, h->S, Sold);
-    L.out4 = Snew;
-    run_stage(h, kg::ST_P2_S1B, L);
     set_in(L, g, h->S, Snew);
     L.out = h->U;
     L.skip_last_i = inflow;
@@ -940,14 +960,9 @@ int step_pirk3(kg_solver* h, int nsteps) {
     double2* Snew = fld(h->S, g, 9 - h->s_cur);
     double2* Told = fld(h->T, g, h->t_cur);
     double2* Tnew = fld(h->T, g, 9 - h->t_cur);
+    run_pirk_s1(h, Sold, Snew);
     kg::StageLaunch L = base_launch(h);
-    set_in(L, g, h->U, fld(h->U, g, 4));
     L.base = h->U;
-    L.out = h->S;
-    run_stage(h, kg::ST_P2_S1A, L);
-    set_in(L, g, h->S, Sold);
-    L.out4 = Snew;
-    run_stage(h, kg::ST_P2_S1B, L);
     set_in(L, g, h->S, Snew);
     L.out = h->T;
     run_stage(h, kg::ST_P3_S2A, L);
@@ -1215,6 +1230,61 @@ int step_rk3_bo(kg_solver* h, kg_solver* c, const double2* c_old, double a0, dou
     run_ghost(h, outs[st], h->U, inflow);
     if ((rc = prolong(outs[st], at[st]))) return rc;
   }
+  h->t = h->t + h->dt;
+  KG_CK(cudaGetLastError());
+  return KG_OK;
+}
+
+// PIRK2 / PIRK3 step of a refined level (pirk2, MoL/lines_method_lib.f90:271-332;
+// pirk3, :334-408).  The stage arrays stand at t + dt (u_stage) and t + dt/2
+// (u_stage_2, PIRK3), and their buffer planes take the coarse state
+// interpolated to those times, Pi included.  So the stale-Pi slot that the
+// next step's stage 1 reads holds, on the buffer planes, the coarse Pi at the
+// start of that step: the same role the slot plays on the interior, where it
+// holds this level's own prediction of Pi there.
+int step_pirk_bo(kg_solver* h, kg_solver* c, const double2* c_old, double a0, double da, int nbuf, int order) {
+  int rc;
+  if ((rc = ensure(h, &h->S, 6))) return rc;
+  if (order == 3 && (rc = ensure(h, &h->T, 6))) return rc;
+  const Grid& g = h->g;
+  const int inflow = h->p.bc_rmax == KG_INFLOW;
+  auto prolong = [&](double2* u, double2* upi, double alpha) -> int {
+    Prof pf(h, PK_PROLONG, 1);
+    if (kg::launch_prolong(g, u, c->g, c_old, c->U, alpha, nbuf, h->stream, upi))
+      return set_err(h, KG_EINVAL, "refined level does not fit inside its coarser level");
+    return KG_OK;
+  };
+  if ((rc = prolong(h->U, nullptr, a0))) return rc;
+  double2* Sold = fld(h->S, g, h->s_cur);
+  double2* Snew = fld(h->S, g, 9 - h->s_cur);
+  run_pirk_s1(h, Sold, Snew);
+  if ((rc = prolong(h->S, Snew, a0 + da))) return rc;
+  kg::StageLaunch L = base_launch(h);
+  L.base = h->U;
+  set_in(L, g, h->S, Snew);
+  if (order == 3) {
+    double2* Told = fld(h->T, g, h->t_cur);
+    double2* Tnew = fld(h->T, g, 9 - h->t_cur);
+    L.out = h->T;
+    run_stage(h, kg::ST_P3_S2A, L);
+    set_in(L, g, h->T, Told);
+    L.aux4 = Snew;
+    L.out4 = Tnew;
+    run_stage(h, kg::ST_P3_S2B, L);
+    if ((rc = prolong(h->T, Tnew, a0 + 0.5 * da))) return rc;
+    set_in(L, g, h->T, Tnew);
+    L.out = h->U;
+    L.skip_last_i = inflow;
+    run_stage(h, kg::ST_P3_S3, L);
+    h->t_cur = 9 - h->t_cur;
+  } else {
+    L.out = h->U;
+    L.skip_last_i = inflow;
+    run_stage(h, kg::ST_P2_S2, L);
+  }
+  run_ghost(h, h->U, h->U, inflow);
+  if ((rc = prolong(h->U, nullptr, a0 + da))) return rc;
+  h->s_cur = 9 - h->s_cur;
   h->t = h->t + h->dt;
   KG_CK(cudaGetLastError());
   return KG_OK;
@@ -1856,7 +1926,9 @@ int kg_sph_harmonics(kg_solver* h, int L, double* out) {
 }
 
 int kg_set_kernel_variant(kg_solver* h, int variant) {
-  if (!h || variant < 0 || variant > 2) return KG_EINVAL;
+  if (!h || variant < 0 || variant > 5) return KG_EINVAL;
+  if (variant >= 2 && !kg::tma_available(h->g, h->U))
+    return set_err(h, KG_EINVAL, "tensor maps unavailable for this grid: forms 2-5 need them");
   h->variant = variant;
   h->graph_gen++;
   return KG_OK;
@@ -2333,7 +2405,7 @@ int hier_order(kg_hier* H, kg_solver* from, kg_solver* to, int l) {
   return KG_OK;
 }
 
-// method: 3 = SSP-RK3, 4 = RK4 on every level
+// method: 3 = SSP-RK3, 4 = RK4, 12 = PIRK2, 13 = PIRK3 on every level
 int hier_step(kg_hier* H, int l, double a0, double da, int method) {
   kg_solver* h = H->lv[l];
   const int n = (int)H->lv.size();
@@ -2344,9 +2416,12 @@ int hier_step(kg_hier* H, int l, double a0, double da, int method) {
       return KG_ECUDA;
     }
   }
-  if (l == 0) rc = method == 3 ? step_rk3(h, 1) : step_rk4(h, 1);
+  if (l == 0)
+    rc = method == 3 ? step_rk3(h, 1) : method == 4 ? step_rk4(h, 1) : method == 12 ? step_pirk2(h, 1)
+                                                                              : step_pirk3(h, 1);
   else if (method == 3) rc = step_rk3_bo(h, H->lv[l - 1], H->uold[l - 1], a0, da, H->nbuf);
-  else rc = step_rk4_bo(h, H->lv[l - 1], H->uold[l - 1], a0, da, H->nbuf);
+  else if (method == 4) rc = step_rk4_bo(h, H->lv[l - 1], H->uold[l - 1], a0, da, H->nbuf);
+  else rc = step_pirk_bo(h, H->lv[l - 1], H->uold[l - 1], a0, da, H->nbuf, method == 12 ? 2 : 3);
   if (rc) {
     H->err = h->err;
     return rc;
@@ -2465,6 +2540,8 @@ int hier_run(kg_hier* H, int nsteps, int method) {
 
 int kg_hier_rk4(kg_hier* H, int nsteps) { return hier_run(H, nsteps, 4); }
 int kg_hier_rk3(kg_hier* H, int nsteps) { return hier_run(H, nsteps, 3); }
+int kg_hier_pirk2(kg_hier* H, int nsteps) { return hier_run(H, nsteps, 12); }
+int kg_hier_pirk3(kg_hier* H, int nsteps) { return hier_run(H, nsteps, 13); }
 
 int kg_hier_synchronize(kg_hier* H) {
   if (!H) return KG_EINVAL;

@@ -42,6 +42,11 @@ void launch_stage_march(int kind, const StageLaunch& L, const double* rsg, cudaS
 // TMA-pipelined form (kg_tma.cu); err: device flag set to 1 when a bounded wait runs out.
 // Returns 0, or -1 if the tensor maps cannot be encoded / the kernel cannot be configured.
 int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st);
+// PIRK stage 1 in one kernel (kg_fused.cu): S(1:4) = u + dt rhs(u), Snew = u(5) +
+// dt rhs_pi(S(1:4), Sold); cfg 0: 32 x 8 tiles, 2 CTAs per SM; 1: 32 x 8, 1 CTA per
+// SM; 2: 32 x 12, 1 CTA per SM.  Returns -1 if the tensor maps cannot be encoded.
+int launch_pirk_s1_fused(int cfg, const Grid& g, const Metric& m, int mk, const double2* U, const double2* Sold,
+                         double2* S, double2* Snew, const double* rsg, int* err, cudaStream_t st);
 // true when the driver can encode the tensor maps the TMA form needs for this grid
 bool tma_available(const Grid& g, const double2* some_state);
 // batched (multi-solve) persistent launches of the TMA stage kernel
@@ -90,8 +95,9 @@ int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, cons
                      int tiled, cudaStream_t st);
 void launch_ghost_fill_cfg(const Grid& g, double2* u, cudaStream_t st);
 // Berger-Oliger transfers between radially nested 2:1 levels (kg_refine.cu)
+// uf_pi: where the fine Pi variable lives (nullptr: uf + 4 fs, the 5-variable layout)
 int launch_prolong(const Grid& gf, double2* uf, const Grid& gc, const double2* c_old, const double2* c_new,
-                   double alpha, int nbuf, cudaStream_t st);
+                   double alpha, int nbuf, cudaStream_t st, double2* uf_pi = nullptr);
 int launch_restrict(const Grid& gc, double2* uc, const Grid& gf, const double2* uf, int keep_out, cudaStream_t st);
 void launch_rhs(const Grid& g, const Metric& m, int metric_kind, const double2* const in[5], double2* out,
                 unsigned mask, cudaStream_t st);

@@ -7,7 +7,8 @@
 //   prolongation: the outermost `nbuf` fine planes take coarse values at the
 //     stage time, cubic Lagrange in r, (-c(a-1) + 9 c(a) + 9 c(a+1) - c(a+2)) / 16
 //     at the odd (midpoint) planes, injection at the even ones, and linear in
-//     time between the coarse level's states at t and t + dt_coarse;
+//     time between the coarse level's states at t and t + dt_coarse (the Pi
+//     variable may live in a separate slot, as the PIRK stage arrays keep it);
 //   restriction: every coarse point under the fine level's interior (all but
 //     the last `keep_out` fine planes) takes the coincident fine value.
 #include <cuda_runtime.h>
@@ -25,8 +26,8 @@ __device__ __forceinline__ double2 prolong_r(const Grid& gc, const double2* c, i
   return rmul(1.0 / 16.0, csub(cadd(cadd(cneg(cm), rmul(9.0, c0)), rmul(9.0, c1)), c2v));
 }
 
-__global__ void prolong_kernel(Grid gf, double2* uf, Grid gc, const double2* c_old, const double2* c_new,
-                               double alpha, int nbuf) {
+__global__ void prolong_kernel(Grid gf, double2* uf, double2* uf_pi, Grid gc, const double2* c_old,
+                               const double2* c_new, double alpha, int nbuf) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long n = (long long)nbuf * gf.NJ * gf.NK;
   if (t >= n) return;
@@ -38,7 +39,8 @@ __global__ void prolong_kernel(Grid gf, double2* uf, Grid gc, const double2* c_o
   for (int v = 0; v < 5; ++v) {
     const double2 po = prolong_r(gc, c_old + (long long)v * gc.fs, iif, jj, k);
     const double2 pn = prolong_r(gc, c_new + (long long)v * gc.fs, iif, jj, k);
-    uf[(long long)v * gf.fs + off3(gf, iif, jj, k)] = cadd(rmul(1.0 - alpha, po), rmul(alpha, pn));
+    double2* dst = (v == 4) ? uf_pi : uf + (long long)v * gf.fs;
+    dst[off3(gf, iif, jj, k)] = cadd(rmul(1.0 - alpha, po), rmul(alpha, pn));
   }
 }
 
@@ -57,13 +59,14 @@ __global__ void restrict_kernel(Grid gc, double2* uc, Grid gf, const double2* uf
 }  // namespace
 
 int launch_prolong(const Grid& gf, double2* uf, const Grid& gc, const double2* c_old, const double2* c_new,
-                   double alpha, int nbuf, cudaStream_t st) {
+                   double alpha, int nbuf, cudaStream_t st, double2* uf_pi) {
   // the stencil reaches coarse plane (NI_f - 1) / 2 + 2, which must lie inside the coarse grid
   if (nbuf < 1 || nbuf > gf.NI || gf.NJ != gc.NJ || gf.NK != gc.NK || (gf.NI - 1) / 2 + 2 > gc.NI - 1 ||
       (gf.NI - nbuf) / 2 - 1 < 0)
     return -1;
   const long long n = (long long)nbuf * gf.NJ * gf.NK;
-  prolong_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(gf, uf, gc, c_old, c_new, alpha, nbuf);
+  if (!uf_pi) uf_pi = uf + 4 * gf.fs;
+  prolong_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(gf, uf, uf_pi, gc, c_old, c_new, alpha, nbuf);
   return 0;
 }
 

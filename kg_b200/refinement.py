@@ -81,6 +81,14 @@ class BergerOliger:
         """nsteps coarse SSP-RK3 steps (level l takes 2^l steps per coarse step)"""
         self._ck(self._lib.kg_hier_rk3(self._H, int(nsteps)))
 
+    def pirk2(self, nsteps=1):
+        """nsteps coarse PIRK2 steps (level l takes 2^l steps per coarse step)"""
+        self._ck(self._lib.kg_hier_pirk2(self._H, int(nsteps)))
+
+    def pirk3(self, nsteps=1):
+        """nsteps coarse PIRK3 steps (level l takes 2^l steps per coarse step)"""
+        self._ck(self._lib.kg_hier_pirk3(self._H, int(nsteps)))
+
     def synchronize(self):
         self._ck(self._lib.kg_hier_synchronize(self._H))
 

@@ -20,7 +20,7 @@ def _ic(level_view):
     return smooth_exact(lv.Nx, lv.Ny, lv.Nz, XMIN, lv.params.xmax, amp=1e-3, r0=8.0, width=2.0)
 
 
-@pytest.mark.parametrize("method", ["rk4", "rk3"])
+@pytest.mark.parametrize("method", ["rk4", "rk3", "pirk2", "pirk3"])
 def test_single_level_is_the_plain_solver(method):
     from kg_b200 import ScalarField
     from kg_b200.refinement import BergerOliger
@@ -45,8 +45,9 @@ def _run_bo(nsteps, r_fine, method="rk4"):
     return bo
 
 
-def test_restriction_and_level_clocks():
-    bo = _run_bo(3, (16.0, 9.0))
+@pytest.mark.parametrize("method", ["rk4", "pirk2"])
+def test_restriction_and_level_clocks(method):
+    bo = _run_bo(3, (16.0, 9.0), method)
     dt0 = bo.levels[0].dt
     for l, lv in enumerate(bo.levels):
         assert abs(lv.dt - dt0 / 2 ** l) <= 1e-15 * dt0
@@ -60,7 +61,7 @@ def test_restriction_and_level_clocks():
     bo.close()
 
 
-@pytest.mark.parametrize("method", ["rk4", "rk3"])
+@pytest.mark.parametrize("method", ["rk4", "rk3", "pirk2", "pirk3"])
 def test_refined_level_tracks_the_uniform_fine_solve(method):
     from kg_b200 import ScalarField
     from kg_b200.initial_data import smooth_exact
@@ -84,7 +85,7 @@ def test_refined_level_tracks_the_uniform_fine_solve(method):
     bo.close()
 
 
-@pytest.mark.parametrize("method", ["rk4", "rk3"])
+@pytest.mark.parametrize("method", ["rk4", "rk3", "pirk2", "pirk3"])
 def test_pulse_through_the_interface(method):
     """a pulse that starts next to the coarse-fine interface (r = 16) and runs
     through it: inside the refined level, near the interface, the hierarchy
