@@ -295,22 +295,39 @@ def _wave(d):
             "note": "relative error over requests whose FP64 waveform norm exceeds 1e-10; absolute over all"}
 
 
-def precision_leg(w, device, steps=40, every=10, L=64):
+def two_shells_device(w, device, Nx=None, xmax=None):
+    """The workload's seeded shell (r0 ~ U[8, 15]) plus a second seeded shell
+    centred on the extraction radius r = 50 (same form, seed + 1).  Under the
+    reference dt rule the workload grid steps dt = 4.5e-4 (the pole term
+    e^xmin sin(dtheta/2) dphi binds), so a pulse from r0 <= 15 needs some 8e4
+    steps to reach r = 50; the second shell puts signal at the extraction radius
+    from the first step of a bounded run."""
+    from kg_b200.initial_data import shell_ylm_device
+    Nx = Nx or w["Nx"]
+    xmax = xmax or w["xmax"]
+    u0, _ = shell_ylm_device(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, seed=w["seed"], device=f"cuda:{device}")
+    u1, _ = shell_ylm_device(Nx, w["Ny"], w["Nz"], w["xmin"], xmax, seed=w["seed"] + 1, device=f"cuda:{device}",
+                             r0_range=(50.0, 50.0))
+    u0 += u1
+    del u1
+    return u0
+
+
+def precision_leg(w, device, steps=120, every=10, L=64):
     """The precision form on the workload grid: RK4 with the FP32 stencil RHS and
     FP64 state update plus a split-BF16 tensor-core Y_lm projection (l <= L, every
     shell) every `every` steps, against FP64 RK4 with the FP64 projection, from
-    the same initial data.  Device time (CUDA events) of the steps and of the
-    projections; errors of phi and Pi, of the l <= 8 detector waveforms at
-    r = 12 (inside the shell) and r = 50, and of the last all-shell projection."""
+    the same initial data (two_shells_device).  Device time (CUDA events) of the
+    steps and of the projections; errors of phi and Pi, of the l <= 8 detector
+    waveforms at r = 12 (inside the first shell) and r = 50 (the extraction
+    radius), per mode and in total, and of the last all-shell projection."""
     import torch
     from kg_b200 import ScalarField
-    from kg_b200.initial_data import shell_ylm_device
     runs = {}
     for prec in ("fp64", "mixed"):
         s = ScalarField(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], m=w["m"], device=device,
                         l_max=8, n_det=2)
-        u0, _ = shell_ylm_device(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], seed=w["seed"],
-                                 device=f"cuda:{device}")
+        u0 = two_shells_device(w, device)
         s._ck(s._lib.kg_set_state_device(s.handle, 0, C.c_void_p(u0.data_ptr())))
         s.synchronize()
         del u0
@@ -365,7 +382,9 @@ def precision_leg(w, device, steps=40, every=10, L=64):
         return {"rel_l2": float(np.linalg.norm(got - ref) / n), "max_per_mode_rel": float(per_mode[big].max()),
                 "ref_norm": float(n)}
     return {"workload": f"RK4 on the {w['Nx']}x{w['Ny']}x{w['Nz']} grid, {steps} steps, all-shell Y_lm projection "
-                        f"(l<={L}) every {every} steps; detectors at r = 12 and 50",
+                        f"(l<={L}) every {every} steps; detectors at r = 12 and 50; initial data: the workload "
+                        f"shell plus a seeded shell at r = 50",
+            "steps": steps,
             "fp64_step_gpsu": pts / (a["step_ms"] / 1e3), "mixed_step_gpsu": pts / (b["step_ms"] / 1e3),
             "step_speedup": a["step_ms"] / b["step_ms"],
             "fp64_projection_ms": a["proj_ms"] / (steps // every),
@@ -423,29 +442,43 @@ def c0_leg(device, steps=1000):
             "dt_0.25dr": {k: big[k] for k in ("dt", "t_end", "max_abs_u_end", "bounded")}}
 
 
-def refinement_leg(w, device, steps=10, r_fine=(20.0, 15.0, 10.0)):
+def refinement_leg(w, device, steps=10, r_fine=(20.0, 15.0, 10.0), wave_steps=16):
     """The workload grid as the coarse level of a Berger-Oliger hierarchy with
-    radially nested 2:1 levels inside r < 20 (r_fine), FP64 RK4 and SSP-RK3;
-    level l takes 2^l steps per coarse step.  Rate = interior points x stages x
-    steps summed over levels / device time (CUDA events on the coarse level's
-    stream, which every level's work is ordered back into)."""
+    radially nested 2:1 levels inside r < 20, 15, 10 (r_fine); level l takes 2^l
+    steps per coarse step.
+    * Rates, per stepper (RK4, SSP-RK3, PIRK2, PIRK3): interior points x stages x
+      steps summed over levels / device time (CUDA events on the coarse level's
+      stream, which every level's work is ordered back into).
+    * Waveforms: from the two-shell initial data (two_shells_device), the l <= 8
+      detector a_lm at r = 12 (on the finest level that covers it) and r = 50
+      (coarse level), every coarse step for `wave_steps` steps with RK4 and
+      PIRK2, against a uniformly fine solve (the finest level's dr and dt over
+      r in [1.8, 60], which holds both radii and is far larger than the signal
+      travels in the run) and against the coarse level alone."""
     import torch
+    from kg_b200 import ScalarField
     from kg_b200.refinement import BergerOliger
-    from kg_b200.initial_data import shell_ylm_device
-    bo = BergerOliger(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], r_fine=r_fine, m=w["m"],
-                      device=device, l_max=8)
-    for lv in bo.levels:
-        u0, _ = shell_ylm_device(lv.Nx, lv.Ny, lv.Nz, w["xmin"], lv.params.xmax, seed=w["seed"],
-                                 device=f"cuda:{device}")
+
+    def load(lv, Nx, xmax):
+        u0 = two_shells_device(w, device, Nx=Nx, xmax=xmax)
         lv._ck(lv._lib.kg_set_state_device(lv.handle, 0, C.c_void_p(u0.data_ptr())))
         lv.synchronize()
         del u0
+
+    def make_bo():
+        bo = BergerOliger(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], r_fine=r_fine, m=w["m"],
+                          device=device, l_max=8)
+        for lv in bo.levels:
+            load(lv, lv.Nx, lv.params.xmax)
+        return bo
+
+    bo = make_bo()
     l0 = bo.levels[0]
     stream = torch.cuda.ExternalStream(l0._lib.kg_get_stream(l0.handle), device=f"cuda:{device}")
     out = {"workload": f"coarse level = the workload grid; 2:1 levels inside r < {r_fine}, {steps} coarse steps "
                        f"per stepper",
            "levels": [{"Nx": lv.Nx, "r_outer": lv.params.xmax, "dt": lv.dt} for lv in bo.levels]}
-    for method, stages in (("rk4", 4), ("rk3", 3)):
+    for method, stages in (("rk4", 4), ("rk3", 3), ("pirk2", 2), ("pirk3", 3)):
         getattr(bo, method)(1)
         bo.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -463,6 +496,66 @@ def refinement_leg(w, device, steps=10, r_fine=(20.0, 15.0, 10.0)):
         finite = finite and bool(np.isfinite(lv.mass_scalar()))
     out["finite"] = finite
     bo.close()
+    torch.cuda.empty_cache()
+
+    # waveforms at r = 12 and r = 50
+    r_in, r_ext = 12.0, 50.0
+    nlev = len(r_fine) + 1
+    sub = 2 ** (nlev - 1)
+    waves = {}
+    for method in ("rk4", "pirk2"):
+        bo = make_bo()
+        dt0 = bo.levels[0].dt
+        lin = max(l for l in range(nlev) if l == 0 or r_fine[l - 1] > r_in + 1.0)
+        bo.levels[0].set_detectors([r_in, r_ext])
+        bo.levels[lin].set_detectors([r_in, r_ext if lin == 0 else r_in])
+        hw = []
+        for _ in range(wave_steps):
+            getattr(bo, method)(1)
+            a0 = bo.levels[0].proyector_detectors().copy()
+            ai = bo.levels[lin].proyector_detectors().copy()
+            hw.append(np.stack([ai[0], a0[1]]))
+        finest_dx = bo.levels[-1].dx
+        bo.close()
+        torch.cuda.empty_cache()
+        # the coarse level alone
+        cs = ScalarField(w["Nx"], w["Ny"], w["Nz"], w["xmin"], w["xmax"], w["CFL"], m=w["m"], device=device,
+                         l_max=8, n_det=2)
+        load(cs, w["Nx"], w["xmax"])
+        cs.set_detectors([r_in, r_ext])
+        cw = []
+        for _ in range(wave_steps):
+            getattr(cs, method)(nsteps=1)
+            cw.append(cs.proyector_detectors().copy())
+        cs.close()
+        torch.cuda.empty_cache()
+        # uniformly fine: the finest level's dr and dt over [1.8, 60]
+        nf = int(round((60.0 - w["xmin"]) / finest_dx))
+        xf = w["xmin"] + nf * finest_dx
+        fsv = ScalarField(nf, w["Ny"], w["Nz"], w["xmin"], xf, w["CFL"], m=w["m"], device=device, l_max=8,
+                          n_det=2, dt=dt0 / sub)
+        load(fsv, nf, xf)
+        fsv.set_detectors([r_in, r_ext])
+        fw = []
+        for _ in range(wave_steps):
+            getattr(fsv, method)(nsteps=sub)
+            fw.append(fsv.proyector_detectors().copy())
+        fsv.close()
+        torch.cuda.empty_cache()
+        hw, cw, fw = np.array(hw), np.array(cw), np.array(fw)
+        rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+        waves[method] = {
+            "r12": {"hierarchy_vs_uniform_fine": rel(hw[:, 0], fw[:, 0]),
+                    "coarse_vs_uniform_fine": rel(cw[:, 0], fw[:, 0]), "level": lin,
+                    "ref_norm": float(np.linalg.norm(fw[:, 0]))},
+            "r50": {"hierarchy_vs_uniform_fine": rel(hw[:, 1], fw[:, 1]),
+                    "coarse_vs_uniform_fine": rel(cw[:, 1], fw[:, 1]),
+                    "hierarchy_vs_coarse": rel(hw[:, 1], cw[:, 1]), "level": 0,
+                    "ref_norm": float(np.linalg.norm(fw[:, 1]))},
+            "uniform_fine": {"Nx": nf, "r": [w["xmin"], xf], "dt": dt0 / sub}}
+    out["waveforms"] = dict(waves, steps=wave_steps,
+                            note="l <= 8 a_lm at each coarse step, relative L2 over all samples and modes; initial "
+                                 "data: the workload shell plus a seeded shell at r = 50")
     return out
 
 
@@ -588,9 +681,12 @@ def summarize(line, steps):
                             "wave_r50_rel_err": g(p, "waveform_r50", "rel_l2"), "steps": p.get("steps")}
     if "refinement" in line:
         r = line["refinement"]
-        out["refinement_ggpsu"] = {k: r[k]["gpsu"] / 1e9 for k in ("rk4", "rk3", "pirk2") if k in r}
-        if "waveform_r50" in r:
-            out["refinement_wave_r50_rel_err"] = g(r, "waveform_r50", "rel_l2")
+        out["refinement_ggpsu"] = {k: r[k]["gpsu"] / 1e9 for k in ("rk4", "rk3", "pirk2", "pirk3") if k in r}
+        if "waveforms" in r:
+            out["refinement_waveform_rel_err"] = {
+                m: {rad: {k: g(r, "waveforms", m, rad, k) for k in ("hierarchy_vs_uniform_fine",
+                                                                     "coarse_vs_uniform_fine")}
+                    for rad in ("r12", "r50")} for m in ("rk4", "pirk2")}
     if "c0_configured" in line:
         out["c0_ms_per_step"] = line["c0_configured"]["ms_per_step"]
     if "batching" in line:

@@ -1,7 +1,13 @@
 """GPU tests of the configured method (fourth-order differences, sixth-order
 Kreiss-Oliger dissipation, Sommerfeld outer plane, parity-correct pole ghosts;
-RK4): bit-exact against the oracle's restatement, and fourth-order
-self-convergence across three resolutions."""
+RK4): against the oracle's restatement, and fourth-order self-convergence
+across three resolutions.
+
+The method has no reference arithmetic to reproduce, so its kernels contract
+multiply-adds (FMA) while the oracle rounds every product and sum separately.
+The two then differ by a few units in the last place per operation; the tests
+hold the GPU to the oracle within REL = 1e-13 relative L2 over 10 RK4 steps
+(and 1e-12 of max |u| pointwise)."""
 import math
 
 import numpy as np
@@ -26,16 +32,27 @@ def _pair(Nx, Ny, Nz, eps=0.02, m=0.2, steps=10):
     return dev, ora
 
 
+REL = 1e-13
+
+
+def _close(a, b):
+    rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+    return rel <= REL and np.abs(a - b).max() <= 1e-12 * np.abs(b).max(), rel
+
+
 @pytest.mark.parametrize("grid", [(24, 17, 33), (37, 13, 25)])
-def test_configured_rk4_bitexact_vs_oracle(grid):
+def test_configured_rk4_vs_oracle(grid):
     dev, ora = _pair(*grid)
-    assert np.array_equal(dev.u, ora.get_state())
+    assert np.array_equal(dev.u, ora.get_state())   # the ghost fills copy values
     dev.rk4(nsteps=1)
     ora.rk4(1)
-    assert np.array_equal(dev.u, ora.get_state())
+    ok, rel = _close(dev.u, ora.get_state())
+    assert ok, rel
     dev.rk4(nsteps=9)   # graph replay of step pairs
     ora.rk4(9)
-    assert np.array_equal(dev.u, ora.get_state())
+    ok, rel = _close(dev.u, ora.get_state())
+    print(f"configured RK4 x10 on {grid}: rel L2 vs oracle {rel:.2e}")
+    assert ok, rel
 
 
 @pytest.mark.parametrize("grid", [(24, 17, 33), (67, 41, 9), (150, 9, 129)])
@@ -51,7 +68,8 @@ def test_configured_tiled_equals_per_point(grid):
     assert np.array_equal(dev.u, ref.u)
     if grid == (24, 17, 33):
         ora.rk4(3)
-        assert np.array_equal(dev.u, ora.get_state())
+        ok, rel = _close(dev.u, ora.get_state())
+        assert ok, rel
 
 
 def test_configured_scheme_guards():
