@@ -450,8 +450,8 @@ def refinement_leg(w, device, steps=10, r_fine=(20.0, 15.0, 10.0), wave_steps=16
       steps summed over levels / device time (CUDA events on the coarse level's
       stream, which every level's work is ordered back into).
     * Waveforms: from the two-shell initial data (two_shells_device), the l <= 8
-      detector a_lm at r = 12 (on the finest level that covers it) and r = 50
-      (coarse level), every coarse step for `wave_steps` steps with RK4 and
+      detector a_lm at r ~ 12 (on the finest level that covers it) and r ~ 50
+      (coarse level), both on a coarse vertex, every coarse step for `wave_steps` steps with RK4 and
       PIRK2, against a uniformly fine solve (the finest level's dr and dt over
       r in [1.8, 60], which holds both radii and is far larger than the signal
       travels in the run) and against the coarse level alone."""
@@ -498,8 +498,13 @@ def refinement_leg(w, device, steps=10, r_fine=(20.0, 15.0, 10.0), wave_steps=16
     bo.close()
     torch.cuda.empty_cache()
 
-    # waveforms at r = 12 and r = 50
-    r_in, r_ext = 12.0, 50.0
+    # waveforms at r ~ 12 and r ~ 50, on a vertex of the coarse grid, which is a
+    # vertex of every finer grid too: the detectors take the vertex at or below
+    # their radius without radial interpolation (the reference's index search),
+    # so all runs sample the same radius
+    dx0 = (w["xmax"] - w["xmin"]) / w["Nx"]
+    on_vertex = lambda r: w["xmin"] + round((r - w["xmin"]) / dx0) * dx0 + 1e-6 * dx0
+    r_in, r_ext = on_vertex(12.0), on_vertex(50.0)
     nlev = len(r_fine) + 1
     sub = 2 ** (nlev - 1)
     waves = {}
@@ -545,6 +550,7 @@ def refinement_leg(w, device, steps=10, r_fine=(20.0, 15.0, 10.0), wave_steps=16
         hw, cw, fw = np.array(hw), np.array(cw), np.array(fw)
         rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
         waves[method] = {
+            "radii": [r_in, r_ext],
             "r12": {"hierarchy_vs_uniform_fine": rel(hw[:, 0], fw[:, 0]),
                     "coarse_vs_uniform_fine": rel(cw[:, 0], fw[:, 0]), "level": lin,
                     "ref_norm": float(np.linalg.norm(fw[:, 0]))},

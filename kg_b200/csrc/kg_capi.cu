@@ -65,7 +65,7 @@ struct kg_solver {
   double* partials = nullptr;            // mass partial sums + result
   int s_cur = 4, t_cur = 4;              // slot holding the current Pi stage value
   int variant = 2;                       // 0: per-point, 1: 2.5-D marching, 2..5: TMA-pipelined marching
-                                         // (2, 4, 5: PIRK stage 1 fused in one kernel; 3: two launches)
+                                         // (3, 4, 5: PIRK stage 1 fused in one kernel; 2: two launches)
   int* derr = nullptr;                   // device flag: a bounded wait in a kernel ran out
   // CUDA graphs of two consecutive steps per stepper and Pi-slot state
   int use_graphs = 1;
@@ -753,10 +753,10 @@ void set_in(kg::StageLaunch& L, const Grid& g, double2* b0, double2* b4) {
 
 // PIRK stage 1 (pirk2 :278-289, pirk3 :341-352): u_stage(1:4) from u, then
 // u_stage(5) from u_stage(1:4) and the previous step's Pi in Sold; one fused
-// kernel for the TMA forms 2, 4 and 5, two launches otherwise
+// kernel for the TMA forms 3, 4 and 5, two launches otherwise
 void run_pirk_s1(kg_solver* h, double2* Sold, double2* Snew) {
   const Grid& g = h->g;
-  const int cfg = h->variant == 2 ? 0 : h->variant == 4 ? 1 : h->variant == 5 ? 2 : -1;
+  const int cfg = h->variant == 3 ? 0 : h->variant == 4 ? 1 : h->variant == 5 ? 2 : -1;
   if (cfg >= 0) {
     Prof pf(h, PK_S1_FUSED, 1);
     const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
@@ -1609,8 +1609,9 @@ int project_all(kg_solver* h, int L, int precision, double2** out_alm) {
   const int K = Ny * Nz;
   const int Kp = kg::ylm_gemm_pad_k(K), Mp = kg::ylm_gemm_pad_m(2 * Nx), Np = kg::ylm_gemm_pad_n(2 * Nm);
   const size_t nalm = (size_t)(L + 1) * (2 * L + 1) * Nx;
-  // buffer plan: Ahi, Alo (Mp x Kp bf16), Bhi, Blo (Np x Kp), C (Mp x Np f32), F (Nx K c128), alm
-  const size_t szA = (size_t)Mp * Kp * 2, szB = (size_t)Np * Kp * 2, szC = (size_t)Mp * Np * 4;
+  // buffer plan: Ahi, Alo (Mp x Kp bf16), Bhi, Blo (Np x Kp), C (nsplit x Mp x Np f32), F (Nx K c128), alm
+  const int nsplit = kg::ylm_gemm_splits(Kp);
+  const size_t szA = (size_t)Mp * Kp * 2, szB = (size_t)Np * Kp * 2, szC = (size_t)nsplit * Mp * Np * 4;
   const size_t szF = (size_t)Nx * K * 16, szAlm = nalm * 16;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t need = 2 * al(szA) + 2 * al(szB) + al(szC) + al(szF) + al(szAlm);
@@ -1678,7 +1679,7 @@ int project_all(kg_solver* h, int L, int precision, double2** out_alm) {
     }
     {
       Prof pf(h, PK_YLM_PREP, 1);
-      kg::launch_ylm_assemble(Cm, Np, Nx, L, dydz, dalm, h->stream);
+      kg::launch_ylm_assemble(Cm, Np, (long long)Mp * Np, nsplit, Nx, L, dydz, dalm, h->stream);
     }
   } else {
     {

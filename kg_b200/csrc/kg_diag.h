@@ -40,7 +40,8 @@ void launch_shells_to_a(const Grid& g, const double2* u, const ShellInterp& si, 
                         __nv_bfloat16* Ahi, __nv_bfloat16* Alo, double2* F, cudaStream_t st);
 void launch_ylm_b(int L, int Ny, int Nz, int Kp, const double* normP, const double* cosm, const double* sinm,
                   const double* sint, __nv_bfloat16* Bhi, __nv_bfloat16* Blo, cudaStream_t st);
-void launch_ylm_assemble(const float* C, int ldc, int Nx, int L, double dydz, double2* alm, cudaStream_t st);
+void launch_ylm_assemble(const float* C, int ldc, long long csplit, int nsplit, int Nx, int L, double dydz,
+                         double2* alm, cudaStream_t st);
 void launch_ylm_fp64(const double2* F, int Nx, int L, int Ny, int Nz, const double* normP, const double* cosm,
                      const double* sinm, const double* sint, double dydz, double2* alm, cudaStream_t st);
 

@@ -57,6 +57,7 @@ int launch_batch_tma(int kind, int mk, const void* d_items, int n_solves, int n_
 int ylm_gemm_pad_m(int rows);
 int ylm_gemm_pad_n(int cols);
 int ylm_gemm_pad_k(int k);
+int ylm_gemm_splits(int Kp);  // K ranges of the split-K GEMM (FP32 partial tiles added in FP64)
 // batched ghost fill: one launch pair for many solves
 struct GhostDesc {
   Grid g;

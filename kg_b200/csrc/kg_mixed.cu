@@ -295,6 +295,23 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
     mbar_expect_tx(&bars[s], (uint32_t)(STAGE_E * sizeof(TIN)));
     tma_load_4d(ring + (size_t)s * slot_e<TIN>(), tinp, 2 * (ii0 - RH), jj0 - 1, plane_of(t), 0, &bars[s]);
   };
+  // the first planes are requested before the metric tile is loaded, so the
+  // copies are in flight while the tile loads (the ring is free: every warp
+  // finished the previous item before this one started)
+  auto prefetch = [&](int k) {
+    if (k >= k1) return;
+    if (a.npf > 0) tma_prefetch_4d(tp0p, 2 * ii0, jj0, k, 0);
+    if (a.npf > 1) tma_prefetch_4d(tp1p, 2 * ii0, jj0, k, 0);
+  };
+  int nissued = 0;
+  if (tid == 0) {
+    for (int t = 0; t < NST && t < nplanes; ++t) {
+      issue(t);
+      nissued = t + 1;
+    }
+    prefetch(k0);
+    prefetch(k0 + 1);
+  }
   for (int t = tid; t < MT_N; t += TI * TJ) {
     const int mx = t % MW, my = t / MW;
     const int gi = ii0 - RH + mx, gj = jj0 - 1 + my;
@@ -311,20 +328,6 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
       for (int w = 0; w < MT_COUNT; ++w) mtf[w * MT_N + t] = (float)mt[w * MT_N + t];
   }
   __syncthreads();
-  auto prefetch = [&](int k) {
-    if (k >= k1) return;
-    if (a.npf > 0) tma_prefetch_4d(tp0p, 2 * ii0, jj0, k, 0);
-    if (a.npf > 1) tma_prefetch_4d(tp1p, 2 * ii0, jj0, k, 0);
-  };
-  int nissued = 0;
-  if (tid == 0) {
-    for (int t = 0; t < NST && t < nplanes; ++t) {
-      issue(t);
-      nissued = t + 1;
-    }
-    prefetch(k0);
-    prefetch(k0 + 1);
-  }
   // own-point metric: alpha, beta, d_r beta, sqrt(gamma), 1/sqrt(gamma), alpha m^2, phi-flux factors
   double own[9] = {0, 0, 0, 1, 1, 0, 0, 0, 0};
   if (act) {

@@ -128,21 +128,9 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
     tma_load_4d(dst + 4 * FIELD_D, tm1p, 2 * (ii0 - RH), jj0 - 1, z, 0, b);
   };
 
-  // metric tile (phi-independent), zero outside the array
-  for (int t = tid; t < MT_N; t += TI * TJ) {
-    const int mx = t % MW, my = t / MW;
-    const int gi = ii0 - RH + mx, gj = jj0 - 1 + my;
-    const bool in = gi >= 0 && gi < g.NI && gj >= 0 && gj < g.NJ;
-    const int q = in ? off2(g, gi, gj) : 0;
-    mt[MT_AL * MT_N + t] = in ? ldm(M.alpha, q) : 0.0;
-    mt[MT_BE * MT_N + t] = in ? ldm(M.beta, q) : 0.0;
-    mt[MT_A * MT_N + t] = in ? ldm(MK == MK_KS ? M.asg : M.asg_grr, q) : 0.0;
-    mt[MT_GRR * MT_N + t] = in ? ldm(M.grr, q) : 0.0;
-    mt[MT_GRP * MT_N + t] = in ? ldm(M.grp, q) : 0.0;
-    mt[MT_SG * MT_N + t] = in ? ldm(M.sqrtg, q) : 0.0;
-    mt[MT_HT * MT_N + t] = in ? ldm(M.asg_gtt, q) : 0.0;
-  }
-  __syncthreads();
+  // the first planes are requested before the metric tile is loaded, so the
+  // copies are in flight while the tile loads (the ring is free: every warp
+  // finished the previous item before this one started)
   // the point-wise operands (u_p, accumulator, ...) of plane k are pulled into
   // L2 two planes ahead, so their loads in the combination hit L2
   auto prefetch = [&](int k) {
@@ -160,6 +148,21 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
     prefetch(k0 + 1);
   }
 
+  // metric tile (phi-independent), zero outside the array
+  for (int t = tid; t < MT_N; t += TI * TJ) {
+    const int mx = t % MW, my = t / MW;
+    const int gi = ii0 - RH + mx, gj = jj0 - 1 + my;
+    const bool in = gi >= 0 && gi < g.NI && gj >= 0 && gj < g.NJ;
+    const int q = in ? off2(g, gi, gj) : 0;
+    mt[MT_AL * MT_N + t] = in ? ldm(M.alpha, q) : 0.0;
+    mt[MT_BE * MT_N + t] = in ? ldm(M.beta, q) : 0.0;
+    mt[MT_A * MT_N + t] = in ? ldm(MK == MK_KS ? M.asg : M.asg_grr, q) : 0.0;
+    mt[MT_GRR * MT_N + t] = in ? ldm(M.grr, q) : 0.0;
+    mt[MT_GRP * MT_N + t] = in ? ldm(M.grp, q) : 0.0;
+    mt[MT_SG * MT_N + t] = in ? ldm(M.sqrtg, q) : 0.0;
+    mt[MT_HT * MT_N + t] = in ? ldm(M.asg_gtt, q) : 0.0;
+  }
+  __syncthreads();
   // own-point metric
   const int q = act ? off2(g, ii, jj) : 0;
   double al = 0, be = 0, dxb = 0, sg = 1, rs = 1, am2 = 0, fa = 0, fgrp = 0, fgpp = 0;

@@ -16,7 +16,13 @@
 // hi.hi + hi.lo + lo.hi, all accumulated in FP32 -- three passes of the same
 // BF16 GEMM over K, the dropped lo.lo term being of order 2^-16.
 //
-// GEMM kernel: one CTA per 128 x 256 output tile, 4 warps.  Warp 0 lane 0
+// Split K: each CTA sums the three passes over one range of at most KB_SPLIT
+// K-slices of 64 (3072 sphere points) into its own FP32 partial tile, and the
+// assembly adds the partials in FP64.  A single FP32 accumulator over the whole
+// K = 33153 of the 129 x 257 sphere took some 6000 accumulation steps and
+// carried an error near 1e-4 of the shell norm; per split it is ~20x shorter.
+//
+// GEMM kernel: one CTA per 128 x 256 output tile and K range, 4 warps.  Warp 0 lane 0
 // feeds a 4-deep shared-memory ring with TMA (cp.async.bulk.tensor 2-D,
 // 128-byte swizzle, K-major 64-element slices); warp 1 lane 0 issues
 // tcgen05.mma (kind::f16, M=128, N=256, K=16 per instruction) into a TMEM
@@ -36,6 +42,7 @@ namespace kg {
 namespace {
 
 constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+constexpr int KB_SPLIT = 48;  // K-slices per CTA
 constexpr int A_TILE_B = BM * BK * 2;  // 16 KB
 constexpr int B_TILE_B = BN * BK * 2;  // 32 KB
 constexpr int STAGE_B = A_TILE_B + B_TILE_B;
@@ -99,12 +106,14 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 
 }  // namespace
 
-// C (M' x ldc, FP32, row-major) = sum over three passes of A_p (M' x K) B_p^T,
-// pass 0: (Ahi, Bhi), 1: (Ahi, Blo), 2: (Alo, Bhi); A and B K-major BF16.
+// C_z (M' x ldc, FP32, row-major) = sum over three passes of A_p B_p^T over
+// the K-slices [z KB_SPLIT, (z+1) KB_SPLIT) of split z = blockIdx.z, pass 0:
+// (Ahi, Bhi), 1: (Ahi, Blo), 2: (Alo, Bhi); A and B K-major BF16; the split
+// partials C_z lie csplit floats apart.
 __global__ void __launch_bounds__(128, 1)
     ylm_gemm_kernel(const __grid_constant__ CUtensorMap tAhi, const __grid_constant__ CUtensorMap tAlo,
                     const __grid_constant__ CUtensorMap tBhi, const __grid_constant__ CUtensorMap tBlo, float* C,
-                    int ldc, int Mrows, int Ncols, int K, int* err) {
+                    int ldc, int Mrows, int Ncols, int K, long long csplit, int* err) {
   extern __shared__ __align__(1024) unsigned char gsm[];
   unsigned char* base = gsm + ((1024u - (saddr(gsm) & 1023u)) & 1023u);
   uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)STAGES * STAGE_B);
@@ -113,8 +122,10 @@ __global__ void __launch_bounds__(128, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  const int nk = K / BK;
+  const int kb0 = blockIdx.z * KB_SPLIT;
+  const int nk = min(K / BK - kb0, KB_SPLIT);  // K-slices of this split (>= 1 by the launch)
   const int total = 3 * nk;
+  C += (long long)blockIdx.z * csplit;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tmem_slot)),
@@ -144,7 +155,7 @@ __global__ void __launch_bounds__(128, 1)
         bad = 1;
         break;
       }
-      const int pass = it / nk, kb = it % nk;
+      const int pass = it / nk, kb = kb0 + it % nk;
       unsigned char* sa = base + (size_t)s * STAGE_B;
       unsigned char* sb = sa + A_TILE_B;
       mbar_expect_tx(&full[s], STAGE_B);
@@ -274,8 +285,8 @@ __global__ void ylm_b_kernel(int L, int Ny, int Nz, int Kp, const double* __rest
 }
 
 // a_lm(l, m, shell) from the GEMM blocks P Q / R T
-__global__ void ylm_assemble_kernel(const float* __restrict__ C, int ldc, int Nx, int L, double dydz,
-                                    double2* __restrict__ alm) {
+__global__ void ylm_assemble_kernel(const float* __restrict__ C, int ldc, long long csplit, int nsplit, int Nx,
+                                    int L, double dydz, double2* __restrict__ alm) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int NL = L + 1, NM = 2 * L + 1;
   const long long n = (long long)NL * NM * Nx;
@@ -289,8 +300,14 @@ __global__ void ylm_assemble_kernel(const float* __restrict__ C, int ldc, int Nx
     const int am = m < 0 ? -m : m;
     const int Nm = (L + 1) * (L + 2) / 2;
     const int mode = l * (l + 1) / 2 + am;
-    const double P = C[(size_t)iv * ldc + mode], Q = C[(size_t)iv * ldc + Nm + mode];
-    const double R = C[(size_t)(Nx + iv) * ldc + mode], T = C[(size_t)(Nx + iv) * ldc + Nm + mode];
+    double P = 0.0, Q = 0.0, R = 0.0, T = 0.0;  // the split partials added in FP64, in split order
+    for (int z = 0; z < nsplit; ++z) {
+      const float* Cz = C + (long long)z * csplit;
+      P += (double)Cz[(size_t)iv * ldc + mode];
+      Q += (double)Cz[(size_t)iv * ldc + Nm + mode];
+      R += (double)Cz[(size_t)(Nx + iv) * ldc + mode];
+      T += (double)Cz[(size_t)(Nx + iv) * ldc + Nm + mode];
+    }
     if (m >= 0) out = c2(P + T, R - Q);
     else {
       const double sg = (am & 1) ? -1.0 : 1.0;
@@ -407,8 +424,10 @@ bool map_kmajor(CUtensorMap* tm, const __nv_bfloat16* p, int Kp, int rows, int b
 int ylm_gemm_pad_m(int rows) { return (rows + BM - 1) / BM * BM; }
 int ylm_gemm_pad_n(int cols) { return (cols + BN - 1) / BN * BN; }
 int ylm_gemm_pad_k(int k) { return (k + BK - 1) / BK * BK; }
+int ylm_gemm_splits(int Kp) { return (Kp / BK + KB_SPLIT - 1) / KB_SPLIT; }
 
-// C (Mp x Np) = three-pass split-BF16 product; all dimensions already padded
+// C_z (Mp x Np each, ylm_gemm_splits(Kp) of them, back to back) = three-pass
+// split-BF16 product over split z's K range; all dimensions already padded
 int launch_ylm_gemm(const __nv_bfloat16* Ahi, const __nv_bfloat16* Alo, const __nv_bfloat16* Bhi,
                     const __nv_bfloat16* Blo, float* C, int Mp, int Np, int Kp, int* err, cudaStream_t st) {
   CUtensorMap a0, a1, b0, b1;
@@ -422,7 +441,8 @@ int launch_ylm_gemm(const __nv_bfloat16* Ahi, const __nv_bfloat16* Alo, const __
       return -1;
     attr = true;
   }
-  ylm_gemm_kernel<<<dim3(Np / BN, Mp / BM), 128, GEMM_SMEM, st>>>(a0, a1, b0, b1, C, Np, Mp, Np, Kp, err);
+  ylm_gemm_kernel<<<dim3(Np / BN, Mp / BM, ylm_gemm_splits(Kp)), 128, GEMM_SMEM, st>>>(
+      a0, a1, b0, b1, C, Np, Mp, Np, Kp, (long long)Mp * Np, err);
   return 0;
 }
 
@@ -439,9 +459,10 @@ void launch_ylm_b(int L, int Ny, int Nz, int Kp, const double* normP, const doub
   ylm_b_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(L, Ny, Nz, Kp, normP, cosm, sinm, sint, Bhi, Blo);
 }
 
-void launch_ylm_assemble(const float* C, int ldc, int Nx, int L, double dydz, double2* alm, cudaStream_t st) {
+void launch_ylm_assemble(const float* C, int ldc, long long csplit, int nsplit, int Nx, int L, double dydz,
+                         double2* alm, cudaStream_t st) {
   const long long n = (long long)(L + 1) * (2 * L + 1) * Nx;
-  ylm_assemble_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(C, ldc, Nx, L, dydz, alm);
+  ylm_assemble_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(C, ldc, csplit, nsplit, Nx, L, dydz, alm);
 }
 
 void launch_ylm_fp64(const double2* F, int Nx, int L, int Ny, int Nz, const double* normP, const double* cosm,

@@ -1,5 +1,6 @@
 """Small, self-contained runs of each kernel family, for profilers.
 
+    python -m kg_b200.profile_cases pirk       [--grid Nx,Ny,Nz] [--steps K] [--variant V]
     python -m kg_b200.profile_cases mixed      [--grid Nx,Ny,Nz] [--steps K]
     python -m kg_b200.profile_cases configured [--grid Nx,Ny,Nz] [--steps K]
     python -m kg_b200.profile_cases batch      [--solves N] [--precision fp64|mixed] [--mix serving|c3] [--steps K]
@@ -9,6 +10,8 @@
 Each case builds seeded synthetic input on the device, runs K steps and exits
 0 (or raises); the sizes default to a few GB of device memory, larger than
 L2, so a profiler capture of one launch is representative and ends quickly.
+  pirk:       PIRK2 of the reference's method on a radial slab of the
+              benchmark grid, in the stage-kernel form V (kg_set_kernel_variant)
   mixed:      RK4 with the FP32 stencil RHS and FP64 update (mixed_rk4_* kernels)
   configured: RK4 of the fourth-order method (cfg_stage_kernel)
   batch:      a request mix advanced as one batch (tma_batch_kernel /
@@ -40,7 +43,8 @@ def _device_ic(s, Nx, Ny, Nz, xmin, xmax, seed=7):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["mixed", "configured", "batch", "refine", "diag"])
+    ap.add_argument("case", choices=["pirk", "mixed", "configured", "batch", "refine", "diag"])
+    ap.add_argument("--variant", type=int, default=2)
     ap.add_argument("--grid", default=None)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--solves", type=int, default=30)
@@ -49,7 +53,16 @@ def main(argv=None):
     ap.add_argument("--kchunk", type=int, default=64)
     a = ap.parse_args(argv)
     from .lines_method import ScalarField
-    if a.case == "mixed":
+    if a.case == "pirk":
+        Nx, Ny, Nz = _grid(a.grid, (512, 129, 257))
+        xmax = 1.8 + 0.1944 * Nx
+        s = ScalarField(Nx, Ny, Nz, 1.8, xmax, 0.25, m=0.3, device=0)
+        _device_ic(s, Nx, Ny, Nz, 1.8, xmax)
+        s._ck(s._lib.kg_set_kernel_variant(s.handle, a.variant))
+        for _ in range(a.steps):
+            s.pirk2(1)
+        s.synchronize()
+    elif a.case == "mixed":
         Nx, Ny, Nz = _grid(a.grid, (384, 129, 257))
         xmax = 1.8 + 0.1944 * Nx
         s = ScalarField(Nx, Ny, Nz, 1.8, xmax, 0.25, m=0.3, device=0)

@@ -5,7 +5,10 @@ detector currents jr/jtheta/jphi_NN.t.asc every save_0d steps) and of savealm
 (IO/save_data.f90:54-110: Harmonic_coeficientsNN.lm.asc every `save` steps).
 Every row read back from the files is compared with the same quantity from the
 oracle, stepped alongside: times exactly, Mass_scalar and currents to 1e-12
-relative, a_lm to 1e-12 of the block's largest coefficient."""
+relative, a_lm to 1e-12 of the block's largest coefficient.  The reference's
+diagnostic integrates rho as it stands (its call to density() is commented
+out, MoL/diagnostic_lib.f90:211), so the driver here refreshes rho with
+density() before each diagnostic, as the oracle's mass does."""
 import os
 
 import numpy as np
@@ -33,6 +36,7 @@ def test_writer_rows_match_the_oracle(tmp_path):
     for l in range(1, nsteps + 1):
         s.pirk2()
         ora.pirk2(1)
+        s.density()
         s.diagnostic(l)
         w.step(l)
         times.append(ora.scalars()["t"])

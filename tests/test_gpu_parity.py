@@ -219,10 +219,9 @@ C1_SLAB = dict(Nx=160, Ny=129, Nz=257, xmin=1.8, xmax=1.8 + 398.2 * 160 / 2048)
 @pytest.mark.parametrize("method,variant", [("pirk2", 2), ("pirk3", 2), ("rk3", 2), ("rk4", 2), ("pirk2", 3),
                                             ("pirk2", 5)])
 def test_benchmark_sphere_steppers_bitexact(method, variant):
-    """Default kernels (variant 2, with the fused PIRK stage 1) on the
-    benchmark's theta x phi grid, 3 steps of each stepper, bit-exact against
-    the oracle (threaded); PIRK2 also with the two-launch stage 1 (variant 3)
-    and the 32 x 12 fused tile (variant 5)."""
+    """Default kernels (variant 2) on the benchmark's theta x phi grid, 3 steps
+    of each stepper, bit-exact against the oracle (threaded); PIRK2 also with
+    the fused stage 1 (variant 3, and variant 5 with 32 x 12 tiles)."""
     from oracle.oracle import set_threads, max_threads
     set_threads(max_threads())
     g = C1_SLAB
@@ -280,8 +279,14 @@ def test_profile_and_launch_count():
     ms = (C.c_double * nk)()
     cnt = (C.c_longlong * nk)()
     dev._ck(dev._lib.kg_profile_read(dev.handle, ms, cnt))
-    # PIRK2 step: fused stage 1, stage 2, two ghost-fill launches
-    assert dev._lib.kg_launch_count(dev.handle) - n0 == 2 * 4
+    # PIRK2 step of the default form: stage 1 (psi, Pi), stage 2, two ghost-fill launches
+    assert dev._lib.kg_launch_count(dev.handle) - n0 == 2 * 5
     assert cnt[2] == 2 and ms[2] > 0.0
+    # the fused stage 1 (form 3): one launch in place of two
+    dev._ck(dev._lib.kg_set_kernel_variant(dev.handle, 3))
+    n0 = dev._lib.kg_launch_count(dev.handle)
+    dev.pirk2(2)
+    dev._ck(dev._lib.kg_profile_read(dev.handle, ms, cnt))
+    assert dev._lib.kg_launch_count(dev.handle) - n0 == 2 * 4
     names = [dev._lib.kg_profile_kind_name(i).decode() for i in range(nk)]
     assert cnt[names.index("stage_pirk_s1_fused")] == 2
