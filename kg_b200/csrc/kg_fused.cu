@@ -268,6 +268,27 @@ __global__ void __launch_bounds__(FI * TJ, MINB)
     av = rmul(g.rdx, av);
     return cadd(cadd(d, rmul(be_c, av)), rmul(dxb_c, f0));
   };
+  // the same for the tile's own columns, whose r neighbours (two on each side)
+  // and alpha at +-1 all lie in the box and the tile: no bounds checks
+  auto psi1_rhs_own = [&](const unsigned char* st, int c, int r, double be_c, double dxb_c) {
+    auto aPi = [&](int cc) { return rmul(MWd(mAL, cc, r), RA(st, G::OFF_A4, cc, r)); };
+    auto ps1 = [&](int cc) { return RA(st, G::OFF_A1, cc, r); };
+    double2 d;
+    if (c == 0) d = fwd3(aPi(0), aPi(1), aPi(2));
+    else if (c == n) d = bwd3(aPi(c), aPi(c - 1), aPi(c - 2));
+    else d = ctr(aPi(c - 1), aPi(c + 1));
+    d = rmul(g.rdx, d);
+    const double2 f0 = ps1(c);
+    double2 av;
+    if (c <= 1) av = fwd3(f0, ps1(c + 1), ps1(c + 2));
+    else if (c == n - 1) av = csub(ps1(c + 1), ps1(c - 1));
+    else if (c == n) av = bwd3(f0, ps1(c - 1), ps1(c - 2));
+    else if (be_c > 0.0) av = fwd3(f0, ps1(c + 1), ps1(c + 2));
+    else if (be_c < 0.0) av = bwd3(f0, ps1(c - 1), ps1(c - 2));
+    else av = csub(ps1(c + 1), ps1(c - 1));
+    av = rmul(g.rdx, av);
+    return cadd(cadd(d, rmul(be_c, av)), rmul(dxb_c, f0));
+  };
   // phi-direction difference of a quantity at plane k from its values at
   // prev(k) and next(k) (the seam planes as the reference writes them)
   auto dphi = [&](int k, double2 vp, double2 vn) {
@@ -373,7 +394,7 @@ __global__ void __launch_bounds__(FI * TJ, MINB)
           EoN = Eown(nx);
         }
         S1 = cadd(RA(cu, G::OFF_A1, ii, jj),
-                  rmul(g.dt, psi1_rhs(cu, p, ii, jj, MTl(mBE + 2 * MW, ii, jj), MTl(mDXB, ii, jj))));
+                  rmul(g.dt, psi1_rhs_own(cu, ii, jj, MWd(mBE, ii, jj), MTl(mDXB, ii, jj))));
         S3 = cadd(RC(cu, ii, jj), rmul(g.dt, dphi(p, EoPv, EoN)));
         const double fa = MTl(mA, ii, jj);  // alpha sqrtg (KS) / alpha gamma^phph (Schw, below)
         F0 = (MK == MK_KS) ? rmul(fa, cadd(rmul(MTl(mGRP, ii, jj), S1), rmul(fgpp, S3))) : rmul(fgpp, S3);
