@@ -205,13 +205,15 @@ def batch_leg(device, steps=5, budget=120e9, count=512):
     waves.append(cur)
     wave = waves[0]
     shapes = sorted({(r.grid()["Nx"], r.grid()["Ny"], r.grid()["Nz"]) for r in wave})
-    tune = autotune(shapes[:: max(1, len(shapes) // 6)], device=device, kchunks=(16, 32, 64), steps=2)
+    sample = shapes[:: max(1, len(shapes) // 6)]
+    tune = {p: autotune(sample, device=device, kchunks=(16, 32, 64), steps=2, precision=p) for p in ("fp64", "mixed")}
     torch.cuda.empty_cache()
     eng = engine_leg(wave, device, tune, steps=steps)
     interior = sum(r.Nr * r.Ntheta * 2 * r.Ntheta for r in wave)
     gpsu = lambda ms: interior * 4 * steps / (ms / 1e3)
     return {"workload": BATCH_DESC, "solves_drawn": count, "waves_for_all": len(waves), "wave_solves": len(wave),
-            "wave_interior_points": interior, "tuning": list(tune), "engine_device_time": eng,
+            "wave_interior_points": interior, "tuning": {p: _tdesc(t) for p, t in tune.items()},
+            "engine_device_time": eng,
             "gpsu": {"plain_fp64": gpsu(eng["plain_fp64_ms"]), "batched_fp64": gpsu(eng["batched_fp64_ms"]),
                      "batched_mixed": gpsu(eng["batched_mixed_ms"])}}
 
@@ -223,15 +225,16 @@ def serve_leg(count, device):
     reqs = draw_requests(seed=20240602, rate=2000.0, count=count, nr=(128, 512), nr_step=64, ntheta=(16, 32),
                          steps=(100, 1000), quantum=10)
     shapes = sorted({(r.grid()["Nx"], r.grid()["Ny"], r.grid()["Nz"]) for r in reqs})
-    tune = autotune(shapes[:: max(1, len(shapes) // 6)], device=device, kchunks=(16, 32, 64), steps=2)
+    sample = shapes[:: max(1, len(shapes) // 6)]
+    tune = {p: autotune(sample, device=device, kchunks=(16, 32, 64), steps=2, precision=p) for p in ("fp64", "mixed")}
     plain = Server(mode="plain", device=device).run(reqs)
-    batched = Server(mode="batched", device=device, tuning=tune).run(reqs)
-    mixed = Server(mode="batched", device=device, tuning=tune, precision="mixed").run(reqs)
+    batched = Server(mode="batched", device=device, tuning=tune["fp64"]).run(reqs)
+    mixed = Server(mode="batched", device=device, tuning=tune["mixed"], precision="mixed").run(reqs)
     strip = lambda d: {k: d[k] for k in ("completed", "wall_s", "solves_per_s", "p50_s", "p99_s") if k in d}
     engine = engine_leg(reqs, device, tune)
     return {"workload": SERVE_DESC, "requests": count, "engine_device_time": engine, "plain_fp64": strip(plain),
-            "batched_fp64": dict(strip(batched), peak_live=batched.get("peak_live"), tuning=list(tune)),
-            "batched_mixed": dict(strip(mixed), peak_live=mixed.get("peak_live")),
+            "batched_fp64": dict(strip(batched), peak_live=batched.get("peak_live"), tuning=_tdesc(tune["fp64"])),
+            "batched_mixed": dict(strip(mixed), peak_live=mixed.get("peak_live"), tuning=_tdesc(tune["mixed"])),
             "speedup_batched_fp64": batched["solves_per_s"] / plain["solves_per_s"],
             "speedup_batched_mixed": mixed["solves_per_s"] / plain["solves_per_s"],
             "waveform_batched_fp64_vs_plain": _wave(waveform_error_detail(batched, plain)),
@@ -264,7 +267,7 @@ def engine_leg(reqs, device, tune, steps=10):
     out = {"steps": steps, "stored_points": pts, "plain_fp64_ms": plain_ms}
     for prec in ("fp64", "mixed"):
         b = Batch(device, precision=prec)
-        b.set_tuning(*tune)
+        b.set_tuning(*tune[prec])
         solves = [_make_solve(r, 8, device) for r in reqs]
         for s in solves:
             b.add(s)
@@ -288,6 +291,15 @@ def engine_leg(reqs, device, tune, steps=10):
     out["speedup_batched_fp64"] = plain_ms / out["batched_fp64_ms"]
     out["speedup_batched_mixed"] = plain_ms / out["batched_mixed_ms"]
     return out
+
+
+def _tdesc(t):
+    """a Tuning as the bench line reports it"""
+    if t.dispatch == 1:
+        form = {0: "one thread per point", 1: "32x8 tiles, register prefetch", 2: "32x8 tiles, TMA ring"}
+        return {"dispatch": "concurrent single-solve launches, one stream per solve",
+                "stage_kernel_form": form.get(t.variant, t.variant)}
+    return {"dispatch": "persistent launch per stage over all solves", "kchunk": t.kchunk, "ctas": t.blocks}
 
 
 def _wave(d):

@@ -261,6 +261,15 @@ int kg_batch_proyector_detectors(kg_batch *b, double *host_alm);
 /* complex values kg_batch_proyector_detectors writes (sum over members) */
 long long kg_batch_alm_count(const kg_batch *b);
 int kg_batch_get_tuning(const kg_batch *b, int *kchunk, int *blocks);
+/* how kg_batch_rk4 runs the members: dispatch 0 = one persistent launch per RK4
+ * stage over all members (default); 1 = each member's own single-solve kernels
+ * on its own stream, all members concurrently, forked from and joined back into
+ * the batch stream (the same bits as kg_rk4 on each member alone).  variant: in
+ * dispatch 1 the members' stage-kernel form (kg_set_kernel_variant), -1 to keep
+ * each member's own; the mixed form takes -1 or 2..5.  The tuner's third and
+ * fourth knobs. */
+int kg_batch_set_dispatch(kg_batch *b, int dispatch, int variant);
+int kg_batch_get_dispatch(const kg_batch *b, int *dispatch, int *variant);
 long long kg_batch_launch_count(const kg_batch *b);
 void *kg_batch_get_stream(const kg_batch *b);
 

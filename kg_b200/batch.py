@@ -7,10 +7,14 @@ fill, and a step is replayed from a CUDA graph (kg_batch_* in
 include/kg_capi.h).  Members keep their handles for state exchange and
 diagnostics.
 
-`autotune` picks the two launch knobs of a batch -- phi planes per work item
-and the number of persistent CTAs -- by timing candidate shapes on scratch
-solves of the same grid shapes, so the live solves are never advanced by the
-tuning itself.
+`autotune` picks how a batch runs by timing candidates on scratch solves of
+the same grid shapes (the live solves are never advanced by the tuning):
+  * dispatch 0, one persistent launch per stage over all members: the phi
+    planes per work item (kchunk) and the number of persistent CTAs;
+  * dispatch 1, every member's own single-solve kernels on its own stream, all
+    members concurrently: the stage-kernel form, i.e. the tile shape of the
+    stage kernels (32 x 8 (r, theta) tiles fed by TMA, 32 x 8 tiles with
+    register prefetch, or one thread per point in rows of 128).
 """
 from __future__ import annotations
 
@@ -88,13 +92,15 @@ class Batch:
             off += a * b * c
         return res
 
-    def set_tuning(self, kchunk, blocks):
+    def set_tuning(self, kchunk, blocks, dispatch=0, variant=-1):
         self._ck(self._lib.kg_batch_set_tuning(self._b, int(kchunk), int(blocks)))
+        self._ck(self._lib.kg_batch_set_dispatch(self._b, int(dispatch), int(variant)))
 
     def tuning(self):
-        k, b = C.c_int(0), C.c_int(0)
+        k, b, d, v = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
         self._ck(self._lib.kg_batch_get_tuning(self._b, C.byref(k), C.byref(b)))
-        return k.value, b.value
+        self._ck(self._lib.kg_batch_get_dispatch(self._b, C.byref(d), C.byref(v)))
+        return Tuning(k.value, b.value, d.value, v.value)
 
     @property
     def launch_count(self):
@@ -105,18 +111,42 @@ class Batch:
         return self._lib.kg_batch_get_stream(self._b)
 
 
+class Tuning(tuple):
+    """(kchunk, blocks, dispatch, variant): the arguments of Batch.set_tuning"""
+
+    def __new__(cls, kchunk, blocks, dispatch=0, variant=-1):
+        return super().__new__(cls, (int(kchunk), int(blocks), int(dispatch), int(variant)))
+
+    kchunk = property(lambda self: self[0])
+    blocks = property(lambda self: self[1])
+    dispatch = property(lambda self: self[2])
+    variant = property(lambda self: self[3])
+
+
 _TUNE_CACHE = {}
 
 
-def autotune(shapes, device=-1, kchunks=(16, 24, 32, 48, 64), ctas_per_sm=(1, 2), steps=3, sms=None):
-    """Choose (kchunk, blocks) for a batch of solves with the given grid shapes.
+def candidates(precision="fp64", kchunks=(16, 24, 32, 48, 64), ctas_per_sm=(1, 2), sms=148,
+               variants=(2, 1, 0)):
+    """The tuner's search space: persistent launches over (kchunk, CTAs per SM),
+    and concurrent single-solve launches over the stage-kernel forms (the mixed
+    form has the TMA form only)."""
+    out = [Tuning(kc, cps * sms, 0, -1) for kc in kchunks for cps in ctas_per_sm]
+    out += [Tuning(kchunks[0], sms, 1, v) for v in (variants if precision == "fp64" else (2,))]
+    return out
 
-    shapes: list of (Nx, Ny, Nz).  Candidates are timed on scratch solves with
-    those shapes (zero state; the kernels' cost does not depend on the values),
-    best of `steps` graph-replayed RK4 steps each.  Results are cached per
-    sorted shape list."""
+
+def autotune(shapes, device=-1, kchunks=(16, 24, 32, 48, 64), ctas_per_sm=(1, 2), steps=3, sms=None,
+             precision="fp64", variants=(2, 1, 0)):
+    """Choose how a batch of solves with the given grid shapes runs (a Tuning).
+
+    shapes: list of (Nx, Ny, Nz).  Every candidate of `candidates` is timed on
+    scratch solves with those shapes (zero state; the kernels' cost does not
+    depend on the values), `steps` graph-replayed RK4 steps each after two
+    warm-up steps, in the given precision.  Results are cached per sorted
+    shape list and precision."""
     from .lines_method import ScalarField
-    key = tuple(sorted(shapes))
+    key = (tuple(sorted(shapes)), precision)
     if key in _TUNE_CACHE:
         return _TUNE_CACHE[key]
     import torch
@@ -125,22 +155,23 @@ def autotune(shapes, device=-1, kchunks=(16, 24, 32, 48, 64), ctas_per_sm=(1, 2)
     scratch = [ScalarField(nx, ny, nz, 1.8, 1.8 + 0.1 * nx, 0.25, device=device, n_det=2, l_max=0)
                for (nx, ny, nz) in shapes]
     best = None
-    for kc in kchunks:
-        for cps in ctas_per_sm:
-            b = Batch(device)
-            for s in scratch:
-                b.add(s)
-            b.set_tuning(kc, cps * sms)
-            b.rk4(2)  # builds the work list and the graph
-            b.synchronize()
-            t0 = time.perf_counter()
-            b.rk4(steps)
-            b.synchronize()
-            dt = (time.perf_counter() - t0) / steps
-            if best is None or dt < best[0]:
-                best = (dt, kc, cps * sms)
-            b.close()
+    for cand in candidates(precision, kchunks, ctas_per_sm, sms, variants):
+        b = Batch(device, precision=precision)
+        for s in scratch:
+            b.add(s)
+        b.set_tuning(*cand)
+        b.rk4(2)  # builds the work list and the graphs
+        b.synchronize()
+        t0 = time.perf_counter()
+        b.rk4(steps)
+        b.synchronize()
+        dt = (time.perf_counter() - t0) / steps
+        if best is None or dt < best[0]:
+            best = (dt, cand)
+        for s in scratch:
+            b.remove(s)
+        b.close()
     for s in scratch:
         s.close()
-    _TUNE_CACHE[key] = (best[1], best[2])
-    return _TUNE_CACHE[key]
+    _TUNE_CACHE[key] = best[1]
+    return best[1]

@@ -114,6 +114,8 @@ SIGNATURES = [
     ("kg_hier_pirk3", _I, [_P, _I]),
     ("kg_hier_synchronize", _I, [_P]),
     ("kg_batch_get_tuning", _I, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("kg_batch_set_dispatch", _I, [_P, _I, _I]),
+    ("kg_batch_get_dispatch", _I, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("kg_batch_launch_count", C.c_longlong, [_P]),
     ("kg_batch_get_stream", C.c_void_p, [_P]),
     ("kg_integrate_mass_noalloc", _I, [C.c_void_p, C.c_void_p, _I, _I, _I, C.c_double, C.c_double,

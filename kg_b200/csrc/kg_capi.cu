@@ -1996,6 +1996,12 @@ struct kg_batch {
   cudaEvent_t ev = nullptr;
   double2* pin = nullptr;  // pinned staging of the members' detector a_lm
   size_t pin_cap = 0;
+  // 0: one persistent launch per stage over every member; 1: every member's
+  // own single-solve kernels on its own stream, concurrently (forked from and
+  // joined back into the batch stream); variant: the members' stage-kernel form
+  // in dispatch 1 (-1 keeps each member's own)
+  int dispatch = 0;
+  int variant = -1;
 };
 
 #define KG_BCK(call)                                                        \
@@ -2233,6 +2239,28 @@ int kg_batch_rk4(kg_batch* b, int nsteps) {
   if (!b || nsteps < 0) return KG_EINVAL;
   if (b->members.empty() || nsteps == 0) return KG_OK;
   int rc;
+  if (b->dispatch == 1) {
+    // fork: each member's stream waits for the batch stream's pending work
+    KG_BCK(cudaEventRecord(b->ev, b->stream));
+    for (kg_solver* h : b->members) KG_BCK(cudaStreamWaitEvent(h->stream, b->ev, 0));
+    for (kg_solver* h : b->members) {
+      if (b->variant >= 0 && h->variant != b->variant) {
+        h->variant = b->variant;
+        h->graph_gen++;
+      }
+      rc = b->precision ? run_steps(h, 4, nsteps, step_rk4_mixed) : run_steps(h, 3, nsteps, step_rk4);
+      if (rc) {
+        b->err = h->err;
+        return rc;
+      }
+    }
+    // join: the batch stream (detector sampling, admissions) waits for every member
+    for (kg_solver* h : b->members) {
+      KG_BCK(cudaEventRecord(b->ev, h->stream));
+      KG_BCK(cudaStreamWaitEvent(b->stream, b->ev, 0));
+    }
+    return KG_OK;
+  }
   if (b->dirty && (rc = batch_rebuild(b))) return rc;
   // order after each member's own pending work
   for (kg_solver* h : b->members) {
@@ -2365,6 +2393,24 @@ int kg_batch_set_precision(kg_batch* b, int mode) {
   }
   b->precision = mode;
   b->dirty = true;
+  return KG_OK;
+}
+
+int kg_batch_set_dispatch(kg_batch* b, int dispatch, int variant) {
+  if (!b || dispatch < 0 || dispatch > 1 || variant < -1 || variant > 5) return KG_EINVAL;
+  if (dispatch == 1 && b->precision == 1 && variant >= 0 && variant < 2) {
+    b->err = "the mixed-precision stages have the TMA form only (variant 2..5 or -1)";
+    return KG_EINVAL;
+  }
+  b->dispatch = dispatch;
+  b->variant = variant;
+  return KG_OK;
+}
+
+int kg_batch_get_dispatch(const kg_batch* b, int* dispatch, int* variant) {
+  if (!b) return KG_EINVAL;
+  if (dispatch) *dispatch = b->dispatch;
+  if (variant) *variant = b->variant;
   return KG_OK;
 }
 

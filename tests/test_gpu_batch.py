@@ -78,5 +78,57 @@ def test_batch_membership_changes_and_tuning():
 
 def test_autotune_returns_a_valid_shape():
     from kg_b200.batch import autotune
-    kc, blocks = autotune([(16, 9, 17), (40, 13, 25)], kchunks=(8, 32), ctas_per_sm=(1, 2), steps=1)
-    assert kc in (8, 32) and blocks > 0
+    for prec in ("fp64", "mixed"):
+        t = autotune([(16, 9, 17), (40, 13, 25)], kchunks=(8, 32), ctas_per_sm=(1, 2), steps=1, precision=prec)
+        assert t.blocks > 0 and t.dispatch in (0, 1)
+        if t.dispatch == 0:
+            assert t.kchunk in (8, 32)
+        else:
+            assert t.variant in ((2, 1, 0) if prec == "fp64" else (2,))
+
+
+@pytest.mark.parametrize("variant", [-1, 0, 1, 2])
+def test_concurrent_dispatch_matches_solo(variant):
+    """dispatch 1: every member's own single-solve kernels on its own stream,
+    concurrently; the same bits as each solve stepped alone, in every
+    stage-kernel form, and after membership changes"""
+    from kg_b200.batch import Batch
+    batch = Batch()
+    batch.set_tuning(16, 148, 1, variant)
+    members, solos = [], []
+    for sp in SHAPES:
+        m, _ = _solve(sp)
+        s, _ = _solve(sp)
+        batch.add(m)
+        members.append(m)
+        solos.append(s)
+    batch.rk4(1)
+    batch.rk4(4)
+    for s in solos:
+        s.rk4(nsteps=5)
+    batch.remove(members[0])
+    batch.rk4(2)
+    for s in solos[1:]:
+        s.rk4(nsteps=2)
+    for m, s in zip(members, solos):
+        assert np.array_equal(m.u, s.u)
+        assert m.t == s.t
+    assert batch.tuning().dispatch == 1
+
+
+def test_concurrent_dispatch_mixed_matches_persistent():
+    from kg_b200.batch import Batch
+    out = []
+    for tune in ((16, 148, 0, -1), (16, 148, 1, 2)):
+        batch = Batch(precision="mixed")
+        batch.set_tuning(*tune)
+        ms = []
+        for sp in SHAPES:
+            m, _ = _solve(sp)
+            batch.add(m)
+            ms.append(m)
+        batch.rk4(5)
+        batch.synchronize()
+        out.append([m.u for m in ms])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
