@@ -84,12 +84,13 @@ void launch_density(const Grid& g, const Metric& m, const double2* u, double mas
 // trapezium over i in [0,Nx] (ii in [2, NI-3]), j in [0,Ny], k in [0,Nz] of
 // rho*sqrtg, weights 1/2 on the first and last index of each direction
 static const int MASS_THREADS = 256;
-int mass_blocks(const Grid& g) { return 148 * 8; }
+int mass_blocks(const Grid& g) { return 148 * 4; }  // one wave at 4 CTAs (64 registers) per SM
 
 // Each warp takes whole (theta, phi) rows in turn and its lanes stride along r
-// with four independent loads in flight, so the loads are coalesced and no
-// per-point index division is needed; the block count is fixed, so the partial
-// sums (and the result) do not depend on the device.
+// with eight independent loads of rho (and of sqrt(gamma)) in flight, so the
+// loads are coalesced and no per-point index division is needed; the block
+// count is fixed, so the partial sums (and the result) do not depend on the
+// device.
 __global__ void mass_partial_kernel(Grid g, const double* __restrict__ sqrtg, const double* __restrict__ rho,
                                     double* partials) {
   const int ni = g.NI - 4, nj = g.NJ - 4, nk = g.NK;
@@ -104,18 +105,20 @@ __global__ void mass_partial_kernel(Grid g, const double* __restrict__ sqrtg, co
     if (k == 0 || k == nk - 1) wjk *= 0.5;
     const double* rr = rho + off3(g, 2, jj, k);
     const double* sr = sqrtg + off2(g, 2, jj);
-    for (int a0 = lane; a0 < ni; a0 += 128) {
-      double v[4];
+    for (int a0 = lane; a0 < ni; a0 += 256) {
+      double rv[8], sv[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
+        const int a = a0 + 32 * u;
+        rv[u] = a < ni ? __ldg(rr + a) : 0.0;
+        sv[u] = a < ni ? __ldg(sr + a) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
         const int a = a0 + 32 * u;
         const double w = (a == 0 || a == ni - 1) ? 0.5 * wjk : wjk;
-        v[u] = a < ni ? w * (__ldg(rr + a) * __ldg(sr + a)) : 0.0;
+        acc += w * (rv[u] * sv[u]);
       }
-      acc += v[0];
-      acc += v[1];
-      acc += v[2];
-      acc += v[3];
     }
   }
   acc = block_sum(acc);
