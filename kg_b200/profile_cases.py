@@ -2,6 +2,7 @@
 
     python -m kg_b200.profile_cases pirk       [--grid Nx,Ny,Nz] [--steps K] [--variant V]
     python -m kg_b200.profile_cases mixed      [--grid Nx,Ny,Nz] [--steps K]
+    python -m kg_b200.profile_cases proj       [--grid Nx,Ny,Nz] [--steps K] [--lmax L]
     python -m kg_b200.profile_cases configured [--grid Nx,Ny,Nz] [--steps K]
     python -m kg_b200.profile_cases batch      [--solves N] [--precision fp64|mixed] [--mix serving|c3] [--steps K]
     python -m kg_b200.profile_cases refine     [--grid Nx,Ny,Nz] [--steps K]
@@ -13,6 +14,8 @@ L2, so a profiler capture of one launch is representative and ends quickly.
   pirk:       PIRK2 of the reference's method on a radial slab of the
               benchmark grid, in the stage-kernel form V (kg_set_kernel_variant)
   mixed:      RK4 with the FP32 stencil RHS and FP64 update (mixed_rk4_* kernels)
+  proj:       the all-shell Y_lm projection on the tensor cores, K times
+              (split-BF16 tcgen05 GEMM, ylm_gemm_kernel)
   configured: RK4 of the fourth-order method (cfg_stage_kernel)
   batch:      a request mix advanced as one batch (tma_batch_kernel /
               mx_batch_kernel, persistent over a ragged work list): the serving
@@ -43,7 +46,8 @@ def _device_ic(s, Nx, Ny, Nz, xmin, xmax, seed=7):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["pirk", "mixed", "configured", "batch", "refine", "diag"])
+    ap.add_argument("case", choices=["pirk", "mixed", "proj", "configured", "batch", "refine", "diag"])
+    ap.add_argument("--lmax", type=int, default=64)
     ap.add_argument("--variant", type=int, default=2)
     ap.add_argument("--grid", default=None)
     ap.add_argument("--steps", type=int, default=3)
@@ -61,6 +65,14 @@ def main(argv=None):
         s._ck(s._lib.kg_set_kernel_variant(s.handle, a.variant))
         for _ in range(a.steps):
             s.pirk2(1)
+        s.synchronize()
+    elif a.case == "proj":
+        Nx, Ny, Nz = _grid(a.grid, (1024, 129, 257))
+        xmax = 1.8 + 0.1944 * Nx
+        s = ScalarField(Nx, Ny, Nz, 1.8, xmax, 0.25, m=0.3, device=0)
+        _device_ic(s, Nx, Ny, Nz, 1.8, xmax)
+        for _ in range(a.steps):
+            s.project_all_shells(a.lmax, precision=1)
         s.synchronize()
     elif a.case == "mixed":
         Nx, Ny, Nz = _grid(a.grid, (384, 129, 257))

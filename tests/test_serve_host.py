@@ -122,3 +122,17 @@ def test_request_larger_than_budget_is_refused(served):
                                steps=(10, 10), quantum=10)
     with pytest.raises(RuntimeError):
         serve.Server(mode="batched", hbm_budget=serve._bytes_estimate(reqs[0]) / 2).run(reqs)
+
+
+def test_tuner_candidates_cover_both_dispatches():
+    """the batch tuner's search space (host logic): persistent launches over
+    (kchunk, CTAs per SM) and concurrent single-solve launches over the
+    stage-kernel forms; the mixed form has the TMA form only"""
+    from kg_b200.batch import Tuning, candidates
+    c64 = candidates("fp64", kchunks=(16, 32), ctas_per_sm=(1, 2), sms=148)
+    assert Tuning(16, 148, 0, -1) in c64 and Tuning(32, 296, 0, -1) in c64
+    assert {t.variant for t in c64 if t.dispatch == 1} == {0, 1, 2}
+    cmx = candidates("mixed", kchunks=(16,), ctas_per_sm=(2,), sms=148)
+    assert {t.variant for t in cmx if t.dispatch == 1} == {2}
+    t = Tuning(8, 37, 1, 2)
+    assert (t.kchunk, t.blocks, t.dispatch, t.variant) == (8, 37, 1, 2) and tuple(t) == (8, 37, 1, 2)
