@@ -219,12 +219,12 @@ int kg_profile_kinds(void);
 const char *kg_profile_kind_name(int kind);
 /* total kernel launches issued by the handle since creation */
 long long kg_launch_count(const kg_solver *h);
-/* stage-kernel form: 2 = marching kernels fed by a TMA shared-memory ring
- * (default); 3, 4, 5 = the same with PIRK stage 1 (pirk2 :278-289) fused into
- * one kernel, at 2 CTAs per SM, 1 CTA per SM, and 1 CTA per SM with 32 x 12
- * tiles; 1 = 2.5-D marching kernels with register prefetch; 0 = one thread per
+/* stage-kernel form: 3 (default) = marching kernels fed by a TMA shared-memory
+ * ring, with PIRK stage 1 (pirk2 :278-289) fused into one kernel; 2 = the same
+ * with PIRK stage 1 as two launches; 1 = 2.5-D marching kernels with register
+ * prefetch; 0 = one thread per
  * point with cached neighbour loads.  All give bit-identical results, except
- * that forms 1-5 divide by sqrt(gamma) through a reciprocal product that can be
+ * that forms 1-3 divide by sqrt(gamma) through a reciprocal product that can be
  * one unit off IEEE division for dividends below about 2^-1000 in magnitude
  * (form 0 divides outright).  The configured method
  * (kg_set_scheme) takes 0 for one thread per point and any other value for

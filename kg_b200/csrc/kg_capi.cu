@@ -64,7 +64,7 @@ struct kg_solver {
   double* rho = nullptr;
   double* partials = nullptr;            // mass partial sums + result
   int s_cur = 4, t_cur = 4;              // slot holding the current Pi stage value
-  int variant = 2;                       // 0: per-point, 1: 2.5-D marching, 2..5: TMA-pipelined marching
+  int variant = 3;                       // 0: per-point, 1: 2.5-D marching, 2, 3: TMA-pipelined marching
                                          // (3, 4, 5: PIRK stage 1 fused in one kernel; 2: two launches)
   int* derr = nullptr;                   // device flag: a bounded wait in a kernel ran out
   // CUDA graphs of two consecutive steps per stepper and Pi-slot state
@@ -753,15 +753,14 @@ void set_in(kg::StageLaunch& L, const Grid& g, double2* b0, double2* b4) {
 
 // PIRK stage 1 (pirk2 :278-289, pirk3 :341-352): u_stage(1:4) from u, then
 // u_stage(5) from u_stage(1:4) and the previous step's Pi in Sold; one fused
-// kernel for the TMA forms 3, 4 and 5, two launches otherwise
+// kernel in form 3, two launches otherwise
 void run_pirk_s1(kg_solver* h, double2* Sold, double2* Snew) {
   const Grid& g = h->g;
-  const int cfg = h->variant == 3 ? 0 : h->variant == 4 ? 1 : h->variant == 5 ? 2 : -1;
-  if (cfg >= 0) {
+  if (h->variant == 3) {
     Prof pf(h, PK_S1_FUSED, 1);
     const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
     const int mk = h->p.metric == KG_SCHW_EF ? kg::MK_SCHW : kg::MK_KS;
-    if (kg::launch_pirk_s1_fused(cfg, g, metric_of(h), mk, h->U, Sold, h->S, Snew, rsg, h->derr, h->stream) == 0)
+    if (kg::launch_pirk_s1_fused(g, metric_of(h), mk, h->U, Sold, h->S, Snew, rsg, h->derr, h->stream) == 0)
       return;
     pf.n = 0;
   }
@@ -1927,9 +1926,9 @@ int kg_sph_harmonics(kg_solver* h, int L, double* out) {
 }
 
 int kg_set_kernel_variant(kg_solver* h, int variant) {
-  if (!h || variant < 0 || variant > 5) return KG_EINVAL;
+  if (!h || variant < 0 || variant > 3) return KG_EINVAL;
   if (variant >= 2 && !kg::tma_available(h->g, h->U))
-    return set_err(h, KG_EINVAL, "tensor maps unavailable for this grid: forms 2-5 need them");
+    return set_err(h, KG_EINVAL, "tensor maps unavailable for this grid: forms 2 and 3 need them");
   h->variant = variant;
   h->graph_gen++;
   return KG_OK;
@@ -2397,9 +2396,9 @@ int kg_batch_set_precision(kg_batch* b, int mode) {
 }
 
 int kg_batch_set_dispatch(kg_batch* b, int dispatch, int variant) {
-  if (!b || dispatch < 0 || dispatch > 1 || variant < -1 || variant > 5) return KG_EINVAL;
+  if (!b || dispatch < 0 || dispatch > 1 || variant < -1 || variant > 3) return KG_EINVAL;
   if (dispatch == 1 && b->precision == 1 && variant >= 0 && variant < 2) {
-    b->err = "the mixed-precision stages have the TMA form only (variant 2..5 or -1)";
+    b->err = "the mixed-precision stages have the TMA form only (variant 2, 3 or -1)";
     return KG_EINVAL;
   }
   b->dispatch = dispatch;

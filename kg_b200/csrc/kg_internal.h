@@ -43,10 +43,9 @@ void launch_stage_march(int kind, const StageLaunch& L, const double* rsg, cudaS
 // Returns 0, or -1 if the tensor maps cannot be encoded / the kernel cannot be configured.
 int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st);
 // PIRK stage 1 in one kernel (kg_fused.cu): S(1:4) = u + dt rhs(u), Snew = u(5) +
-// dt rhs_pi(S(1:4), Sold); cfg 0: 32 x 8 tiles, 2 CTAs per SM; 1: 32 x 8, 1 CTA per
-// SM; 2: 32 x 12, 1 CTA per SM.  Returns -1 if the tensor maps cannot be encoded.
-int launch_pirk_s1_fused(int cfg, const Grid& g, const Metric& m, int mk, const double2* U, const double2* Sold,
-                         double2* S, double2* Snew, const double* rsg, int* err, cudaStream_t st);
+// dt rhs_pi(S(1:4), Sold).  Returns -1 if the tensor maps cannot be encoded.
+int launch_pirk_s1_fused(const Grid& g, const Metric& m, int mk, const double2* U, const double2* Sold, double2* S,
+                         double2* Snew, const double* rsg, int* err, cudaStream_t st);
 // true when the driver can encode the tensor maps the TMA form needs for this grid
 bool tma_available(const Grid& g, const double2* some_state);
 // batched (multi-solve) persistent launches of the TMA stage kernel

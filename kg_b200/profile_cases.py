@@ -48,7 +48,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["pirk", "mixed", "proj", "configured", "batch", "refine", "diag"])
     ap.add_argument("--lmax", type=int, default=64)
-    ap.add_argument("--variant", type=int, default=2)
+    ap.add_argument("--variant", type=int, default=3)
     ap.add_argument("--grid", default=None)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--solves", type=int, default=30)

@@ -101,7 +101,7 @@ def test_boundary_faces_bitexact(bc):
         assert np.array_equal(dev.u, ora.get_state()), f"face {face}"
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 @pytest.mark.parametrize("method", ["pirk2", "pirk3", "rk3", "rk4"])
 @pytest.mark.parametrize("metric,bc", [("Kerr_Schild", "outflow"), ("Schw_EF", "outflow"),
                                        ("Kerr_Schild", "inflow")])
@@ -128,17 +128,24 @@ def test_steppers_bitexact(method, metric, bc, variant):
                                   dict(Nx=4, Ny=5, Nz=5, xmin=1.8, xmax=6.0),
                                   dict(Nx=12, Ny=7, Nz=8, xmin=1.8, xmax=9.0),
                                   dict(Nx=28, Ny=18, Nz=70, xmin=1.8, xmax=15.0),
-                                  dict(Nx=92, Ny=20, Nz=9, xmin=1.8, xmax=30.0)])
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+                                  dict(Nx=92, Ny=20, Nz=9, xmin=1.8, xmax=30.0),
+                                  dict(Nx=26, Ny=11, Nz=9, xmin=1.8, xmax=12.0),
+                                  dict(Nx=56, Ny=12, Nz=12, xmin=1.8, xmax=20.0)])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 def test_march_ragged_tiles(grid, variant):
     """Grids whose r, theta and phi extents leave partial tiles and chunks
     (including a last theta tile of one row) stay bit-exact; the smallest grid
     kg_create accepts (Nx = 4, Ny = Nz = 5) and an even Nz, whose pole partner
     plane k + Nz/2 is not a half turn (the reference's index rule), included.
-    Nx = 28 and 92 leave a last r tile of a single column (33 and 97 stored
-    columns), where the fused PIRK stage 1 reaches two columns left of the tile
-    for the backward closure; Ny = 20 puts the last theta row alone in a tile
-    of 8 and of 12 rows; Nz = 70 gives two phi chunks of the fused kernel."""
+    Nx = 28 and 92 leave a last r tile of a single column in 32-column tiles
+    (33 and 97 stored columns); Ny = 20 puts the last theta row alone in a tile
+    of 8 rows; Nz = 70 gives two phi chunks of the fused kernel.  The fused
+    PIRK stage 1 (form 3) tiles r by 30 columns and moves its last tile back to
+    end at the array's last column: Nx = 26 (31 columns) puts column 0 on the
+    left halo lane of that tile, Nx = 56 (61 columns) overlaps it with the
+    previous tile by 29 columns, Nx = 4 and 12 fit in one tile, and Ny = 11
+    and 12 (16 and 17 stored rows) give theta tiles that meet exactly and that
+    overlap by 7 rows."""
     dev, ora = _pair(grid=grid)
     dev._ck(dev._lib.kg_set_kernel_variant(dev.handle, variant))
     from kg_b200.initial_data import shell_ylm
@@ -217,11 +224,11 @@ C1_SLAB = dict(Nx=160, Ny=129, Nz=257, xmin=1.8, xmax=1.8 + 398.2 * 160 / 2048)
 
 
 @pytest.mark.parametrize("method,variant", [("pirk2", 2), ("pirk3", 2), ("rk3", 2), ("rk4", 2), ("pirk2", 3),
-                                            ("pirk2", 5)])
+                                            ("pirk3", 3)])
 def test_benchmark_sphere_steppers_bitexact(method, variant):
-    """Default kernels (variant 2) on the benchmark's theta x phi grid, 3 steps
-    of each stepper, bit-exact against the oracle (threaded); PIRK2 also with
-    the fused stage 1 (variant 3, and variant 5 with 32 x 12 tiles)."""
+    """TMA kernels on the benchmark's theta x phi grid, 3 steps of each stepper,
+    bit-exact against the oracle (threaded): PIRK2 and PIRK3 with stage 1 as two
+    launches (variant 2) and fused (variant 3, the default)."""
     from oracle.oracle import set_threads, max_threads
     set_threads(max_threads())
     g = C1_SLAB
@@ -279,14 +286,15 @@ def test_profile_and_launch_count():
     ms = (C.c_double * nk)()
     cnt = (C.c_longlong * nk)()
     dev._ck(dev._lib.kg_profile_read(dev.handle, ms, cnt))
-    # PIRK2 step of the default form: stage 1 (psi, Pi), stage 2, two ghost-fill launches
-    assert dev._lib.kg_launch_count(dev.handle) - n0 == 2 * 5
+    # PIRK2 step of the default form: the fused stage 1, stage 2, two ghost-fill launches
+    assert dev._lib.kg_launch_count(dev.handle) - n0 == 2 * 4
     assert cnt[2] == 2 and ms[2] > 0.0
-    # the fused stage 1 (form 3): one launch in place of two
-    dev._ck(dev._lib.kg_set_kernel_variant(dev.handle, 3))
+    names = [dev._lib.kg_profile_kind_name(i).decode() for i in range(nk)]
+    assert cnt[names.index("stage_pirk_s1_fused")] == 2
+    # form 2: stage 1 as two launches (psi, Pi)
+    dev._ck(dev._lib.kg_set_kernel_variant(dev.handle, 2))
     n0 = dev._lib.kg_launch_count(dev.handle)
     dev.pirk2(2)
     dev._ck(dev._lib.kg_profile_read(dev.handle, ms, cnt))
-    assert dev._lib.kg_launch_count(dev.handle) - n0 == 2 * 4
-    names = [dev._lib.kg_profile_kind_name(i).decode() for i in range(nk)]
-    assert cnt[names.index("stage_pirk_s1_fused")] == 2
+    assert dev._lib.kg_launch_count(dev.handle) - n0 == 2 * 5
+    assert cnt[0] == 2 and cnt[1] == 2 and cnt[names.index("stage_pirk_s1_fused")] == 0
