@@ -87,7 +87,9 @@ constexpr int OFF_C = OFF_B + rnd128(B_BYTES);
 constexpr int OFF_D = OFF_C + rnd128(C_BYTES);
 constexpr int SLOT = OFF_D + rnd128(D_BYTES);
 constexpr int H_BYTES = H_NR * FL * 16;
-constexpr int MT_DOUBLES = 2 * M_NC * MAB_NR + M_NC * MHT_NR + M_NC * MSG_NR;
+// (two doubles of padding after the sqrtg table: the Pi stage's discarded lanes
+// read one value past it)
+constexpr int MT_DOUBLES = 2 * M_NC * MAB_NR + M_NC * MHT_NR + M_NC * MSG_NR + 2;
 constexpr size_t SMEM = (size_t)NSTF * SLOT + 2 * (size_t)H_BYTES + (size_t)MT_DOUBLES * 8 + NSTF * 8 + 128;
 static_assert(SMEM <= 113 * 1024, "two CTAs per SM");
 
@@ -117,6 +119,10 @@ __device__ __forceinline__ double2 shfl2_up(double2 v, int d) {
 __device__ __forceinline__ double2 shfl2_down(double2 v, int d) {
   return c2(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d));
 }
+template <bool B>
+struct BoolC {
+  static constexpr bool value = B;
+};
 __device__ __forceinline__ unsigned char* falign128(unsigned char* p) {
   const uint32_t a = saddr(p);
   return p + ((128u - (a & 127u)) & 127u);
@@ -145,7 +151,7 @@ __global__ void __launch_bounds__(NTH, 2)
   double* mBE = mAL + M_NC * MAB_NR;
   double* mHT = mBE + M_NC * MAB_NR;
   double* mSG = mHT + M_NC * MHT_NR;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(mSG + M_NC * MSG_NR);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mSG + M_NC * MSG_NR + 2);
   const Grid& g = a.g;
   const Metric& M = a.m;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * FL + tx;
@@ -252,19 +258,25 @@ __global__ void __launch_bounds__(NTH, 2)
     else z = ctr(vp, vn);
     return rmul(g.rdz, z);
   };
-  // rhs_psi1 at this lane's column (all r neighbours lie in the box)
-  auto psi1_rhs = [&](const unsigned char* st) {
+  // rhs_psi1 at this lane's column (all r neighbours lie in the box); FAST:
+  // the warp's columns are all at least two points from an array end and
+  // beta^r > 0 on all of them, so every lane takes the centred derivative and
+  // the forward upwind difference (the branches the general form would take)
+  auto psi1_rhs = [&](const unsigned char* st, auto fastc) {
+    constexpr bool FAST = decltype(fastc)::value;
     const double be = MAB(mBE, 0, 0);
     auto aPi = [&](int dc) { return rmul(MAB(mAL, dc, 0), RA(st, OFF_A4, dc, 0)); };
     auto ps1 = [&](int dc) { return RA(st, OFF_A1, dc, 0); };
     double2 d;
-    if (c == 0) d = fwd3(aPi(0), aPi(1), aPi(2));
+    if (FAST) d = ctr(aPi(-1), aPi(1));
+    else if (c == 0) d = fwd3(aPi(0), aPi(1), aPi(2));
     else if (c == n) d = bwd3(aPi(0), aPi(-1), aPi(-2));
     else d = ctr(aPi(-1), aPi(1));
     d = rmul(g.rdx, d);
     const double2 f0 = ps1(0);
     double2 av;
-    if (c <= 1) av = fwd3(f0, ps1(1), ps1(2));
+    if (FAST) av = fwd3(f0, ps1(1), ps1(2));
+    else if (c <= 1) av = fwd3(f0, ps1(1), ps1(2));
     else if (c == n - 1) av = csub(ps1(1), ps1(-1));
     else if (c == n) av = bwd3(f0, ps1(-1), ps1(-2));
     else if (be > 0.0) av = fwd3(f0, ps1(1), ps1(2));
@@ -293,6 +305,8 @@ __global__ void __launch_bounds__(NTH, 2)
   double2 phinx = c2(0, 0);  // phi of the own point at the next inner plane, loaded a step ahead
   if (own) phinx = ldf(U, pcol + (long long)plane_of(1) * g.plane);
   __syncthreads();  // metric tables
+  const bool ends = (i0 == 0) || (n < i0 + FO);  // the tile holds an array end (block-uniform)
+  const bool fast = __all_sync(0xffffffffu, c >= 2 && c <= n - 2 && MAB(mBE, 0, 0) > 0.0);
 
   // rolling state
   double2 Ep = c2(0, 0), Ec = c2(0, 0);   // E at P[t-1], P[t]
@@ -305,7 +319,13 @@ __global__ void __launch_bounds__(NTH, 2)
   if (!timed_out) Ec = Ebox(ring + (size_t)slot(0) * SLOT, 0);
   bool failed = __syncthreads_or(timed_out) != 0;
 
-  for (int t = 0; t < NP && !failed; ++t) {
+  // One step of the march at ring step t.  EDGE: t is 0 or NP-1 (E from global
+  // memory outside the sequence); INNER: P[t] is one of the chunk's planes
+  // (outputs, G and H); PI: the Pi stage of P[t-1] follows.  The steady state
+  // (INNER and PI, not EDGE) has no branch around its blocks.
+  auto step = [&](int t, auto fastc, auto edgec, auto innerc, auto pic) {
+    constexpr bool FAST = decltype(fastc)::value, EDGE = decltype(edgec)::value;
+    constexpr bool INNER = decltype(innerc)::value, PI_ = decltype(pic)::value;
     // slot t-1 was released by the barrier that ended the previous step
     if (tid == 0 && t >= 1 && t + 2 < NP) {
       issue(t + 2);
@@ -315,35 +335,34 @@ __global__ void __launch_bounds__(NTH, 2)
     timed_out = __any_sync(0xffffffffu, timed_out) ? 1 : 0;
     if (!timed_out) {
       const int p = plane_of(t);
-      const bool inner = (t >= 1 && t <= NP - 2);
       const unsigned char* cu = ring + (size_t)slot(t) * SLOT;
       const double2 En = (t + 1 < NP) ? Ebox(ring + (size_t)slot(t + 1) * SLOT, 0) : c2(0, 0);
       // ---- psi1, psi3 stages and the phi flux F at P[t]
       double2 vp = Ep, vn = En;
-      if (vcol) {
+      if (EDGE && vcol) {
         if (t == 0) {
           vp = Eglob(jj, X1);
           if (k0 == 0) vn = Eglob(jj, g.Nz - 1);  // next(Nz-2) is Nz-1, not plane 0
-        } else if (t == NP - 1) {
+        } else {
           if (k1 - 1 == g.Nz) vp = Eglob(jj, 1);  // prev(2) is plane 1, not Nz
           vn = Eglob(jj, X4);
         }
       }
-      const double2 S1 = cadd(RA(cu, OFF_A1, 0, 0), rmul(g.dt, psi1_rhs(cu)));
+      const double2 S1 = cadd(RA(cu, OFF_A1, 0, 0), rmul(g.dt, psi1_rhs(cu, fastc)));
       const double2 u3 = *reinterpret_cast<const double2*>(cu + OFF_C + (ty * C_NC + tx) * 16);
       const double2 S3 = cadd(u3, rmul(g.dt, dphi(p, vp, vn)));
       const double2 F0 = (MK == MK_KS) ? rmul(fA, cadd(rmul(fgrp, S1), rmul(fgpp, S3))) : rmul(fgpp, S3);
       double2 Gn = c2(0, 0), S0 = c2(0, 0), U4n = c2(0, 0), Hpn = c2(0, 0);
-      if (inner) {
+      if (INNER) {
         Gn = (MK == MK_KS) ? rmul(fA, cadd(rmul(fgrr, S1), rmul(fgrp, S3))) : rmul(fA, S1);
         S0 = cadd(phinx, rmul(g.dt, Ec));
         // psi2 stage and the theta flux H on the lane's column (columns outside
         // the array: never read, and the pole row would read global memory there)
-        const double2 S2 = vcol ? psi2_stage(cu, p, 0) : c2(0, 0);
+        const double2 S2 = (FAST || vcol) ? psi2_stage(cu, p, 0) : c2(0, 0);
         double2* hb = hbuf + (size_t)(t & 1) * H_NR * FL;
         Hst(hb, 0, S2);
-        if (vcol && ty == 0 && j0 >= 1) Hst(hb, -1, psi2_stage(cu, p, -1));
-        if (vcol && ty == FJ - 1 && j0 + FJ < g.NJ) Hst(hb, 1, psi2_stage(cu, p, 1));
+        if ((FAST || vcol) && ty == 0 && j0 >= 1) Hst(hb, -1, psi2_stage(cu, p, -1));
+        if ((FAST || vcol) && ty == FJ - 1 && j0 + FJ < g.NJ) Hst(hb, 1, psi2_stage(cu, p, 1));
         U4n = RA(cu, OFF_A4, 0, 0);
         if (own) {
           const long long o = pcol + (long long)p * g.plane;
@@ -363,49 +382,50 @@ __global__ void __launch_bounds__(NTH, 2)
         }
       }
       // ---- Pi stage of P[t-1]
-      if (t >= 2) {
+      if (PI_) {
         const int pm = plane_of(t - 1);
-        const bool ends = (i0 == 0) || (n < i0 + FO);  // the tile holds an array end (block-uniform)
         const double2 gm1 = shfl2_up(Gc, 1), gp1 = shfl2_down(Gc, 1);
         double2 gm2 = c2(0, 0), gp2 = c2(0, 0);
-        if (ends) {
+        if (!FAST && ends) {
           gm2 = shfl2_up(Gc, 2);
           gp2 = shfl2_down(Gc, 2);
         }
-        if (own) {
-          const double sg = mSG[ty * M_NC + tx + 1], be = MAB(mBE, 0, 0);
-          double2 d;
-          if (c == 0) d = fwd3(Gc, gp1, gp2);
-          else if (c == n) d = bwd3(Gc, gm1, gm2);
-          else d = ctr(gm1, gp1);
-          const double2 r1 = fcdivm(rmul(g.rdx, d), sg, rs);
-          const double2* hp = hbuf + (size_t)((t - 1) & 1) * H_NR * FL;
-          auto Hr = [&](int dr) { return hp[(ty + 1 + dr) * FL + tx]; };
-          double2 tt;
-          if (jj == 0) tt = cadd(cneg(Hr(1)), Hpc);
-          else if (jj == g.NJ - 1) tt = bwd3(Hr(0), Hr(-1), Hr(-2));
-          else tt = ctr(Hr(-1), Hr(1));
-          const double2 r2 = fcdivm(rmul(g.rdy, tt), sg, rs);
-          const double2 z = dphi(pm, Fm2, F0);
-          const double2 r3 = (MK == MK_KS) ? fcdivm(z, sg, rs) : z;
-          auto PD = [&](int dc) {
-            return *reinterpret_cast<const double2*>(cu + OFF_D + (ty * D_NC + (tx - 1 - D_C0 + dc)) * 16);
-          };
-          const double2 r4 = rmul(dxb, PD(0));
-          auto Q = [&](int dc) { return rmul(mSG[ty * M_NC + tx + 1 + dc], PD(dc)); };
-          double2 av;
-          if (c <= 1) av = fwd3(Q(0), Q(1), Q(2));
-          else if (c == n - 1) av = csub(Q(1), Q(-1));
-          else if (c == n) av = bwd3(Q(0), Q(-1), Q(-2));
-          else if (be > 0.0) av = fwd3(Q(0), Q(1), Q(2));
-          else if (be < 0.0) av = bwd3(Q(0), Q(-1), Q(-2));
-          else av = csub(Q(1), Q(-1));
-          av = rmul(g.rdx, av);
-          const double2 r5 = fcdivm(rmul(be, av), sg, rs);
-          const double2 r6 = rmul(am2, S0p);
-          const double2 rr = csub(cadd(cadd(cadd(cadd(r1, r2), r3), r4), r5), r6);
-          a.Snew[pcol + (long long)pm * g.plane] = cadd(U4p, rmul(g.dt, rr));
-        }
+        // the shared-memory reads below stay inside the CTA's window on every lane
+        // (lanes 0 and 31 read one value past the boxes' own columns, never used)
+        const double sg = mSG[ty * M_NC + tx + 1], be = MAB(mBE, 0, 0);
+        double2 d;
+        if (FAST) d = ctr(gm1, gp1);
+        else if (c == 0) d = fwd3(Gc, gp1, gp2);
+        else if (c == n) d = bwd3(Gc, gm1, gm2);
+        else d = ctr(gm1, gp1);
+        const double2 r1 = fcdivm(rmul(g.rdx, d), sg, rs);
+        const double2* hp = hbuf + (size_t)((t - 1) & 1) * H_NR * FL;
+        auto Hr = [&](int dr) { return hp[(ty + 1 + dr) * FL + tx]; };
+        double2 tt;
+        if (jj == 0) tt = cadd(cneg(Hr(1)), Hpc);
+        else if (jj == g.NJ - 1) tt = bwd3(Hr(0), Hr(-1), Hr(-2));
+        else tt = ctr(Hr(-1), Hr(1));
+        const double2 r2 = fcdivm(rmul(g.rdy, tt), sg, rs);
+        const double2 z = dphi(pm, Fm2, F0);
+        const double2 r3 = (MK == MK_KS) ? fcdivm(z, sg, rs) : z;
+        auto PD = [&](int dc) {
+          return *reinterpret_cast<const double2*>(cu + OFF_D + (ty * D_NC + (tx - 1 - D_C0 + dc)) * 16);
+        };
+        const double2 r4 = rmul(dxb, PD(0));
+        auto Q = [&](int dc) { return rmul(mSG[ty * M_NC + tx + 1 + dc], PD(dc)); };
+        double2 av;
+        if (FAST) av = fwd3(Q(0), Q(1), Q(2));
+        else if (c <= 1) av = fwd3(Q(0), Q(1), Q(2));
+        else if (c == n - 1) av = csub(Q(1), Q(-1));
+        else if (c == n) av = bwd3(Q(0), Q(-1), Q(-2));
+        else if (be > 0.0) av = fwd3(Q(0), Q(1), Q(2));
+        else if (be < 0.0) av = bwd3(Q(0), Q(-1), Q(-2));
+        else av = csub(Q(1), Q(-1));
+        av = rmul(g.rdx, av);
+        const double2 r5 = fcdivm(rmul(be, av), sg, rs);
+        const double2 r6 = rmul(am2, S0p);
+        const double2 rr = csub(cadd(cadd(cadd(cadd(r1, r2), r3), r4), r5), r6);
+        if (own) a.Snew[pcol + (long long)pm * g.plane] = cadd(U4p, rmul(g.dt, rr));
       }
       // roll
       Ep = Ec;
@@ -420,7 +440,20 @@ __global__ void __launch_bounds__(NTH, 2)
     // the H rows of P[t] are visible to every warp, and every warp is done
     // with ring slot t, which the next step refills
     failed = __syncthreads_or(timed_out) != 0;
-  }
+  };
+  // P[0]: psi stage only; P[1]: the first own plane; P[2 .. NP-2]: steady
+  // state; P[NP-1]: psi stage and the Pi stage of the last own plane
+  auto march = [&](auto fastc) {
+    const BoolC<false> no;
+    const BoolC<true> yes;
+    // NP >= 3: a chunk holds at least one plane
+    if (!failed) step(0, fastc, yes, no, no);
+    if (!failed) step(1, fastc, no, yes, no);
+    for (int t = 2; t <= NP - 2 && !failed; ++t) step(t, fastc, no, yes, yes);
+    if (!failed) step(NP - 1, fastc, yes, no, yes);
+  };
+  if (fast) march(BoolC<true>());
+  else march(BoolC<false>());
   if (failed) {
     if (tid == 0) {
       atomicExch(a.err, 1);
