@@ -1146,7 +1146,8 @@ int step_rk4_cfg(kg_solver* h, int nsteps) {
       L.out = outs[st];
       {
         Prof pf(h, kg::ST_RK4_1 + st, 1);
-        if (kg::launch_stage_cfg(kinds[st], L, dxb4, coef, rN, h->variant != 0, h->stream))
+        if (kg::launch_stage_cfg(kinds[st], L, dxb4, h->dmet + (size_t)T_RSG * h->NJ * h->PI, coef, rN,
+                                 h->variant != 0, h->stream))
           return set_err(h, KG_ECUDA, "configured stage could not be launched");
       }
       Prof pg(h, PK_GHOST, 2);

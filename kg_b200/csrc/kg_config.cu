@@ -21,7 +21,9 @@
 //     d_theta of a smooth function on the sphere); the theta flux
 //     alpha sqrt(gamma) gamma^thth psi_2 takes the sign of sin(theta), negative
 //     on the ghost rows where the table holds |sqrt(gamma)|.
-// One thread per stored point; neighbours come through the read-only cache.
+// Divisions by sqrt(gamma) and RK4's 1/6 use the correctly rounded reciprocal
+// with one Markstein correction (the IEEE quotient for dividends above about
+// 2^-1000 in magnitude).
 #include <cuda_runtime.h>
 #include "kg_device.cuh"
 #include "kg_internal.h"
@@ -35,6 +37,7 @@ struct CfgArgs {
   Grid g;
   Metric m;
   const double* dxb4;  // D4 d_r beta^r, [jj][ii] with pitch PI
+  const double* rsg;   // 1 / sqrt(gamma), host-rounded, same layout
   const double2* in;   // stage input (5 variables, stride g.fs)
   const double2* base; // u^n
   double2* acc;
@@ -44,10 +47,13 @@ struct CfgArgs {
   double rN;           // r of the outermost stored plane
 };
 
+// plane d steps from plane k (1 <= k <= Nz-1) over the Nz-1 distinct planes 1..Nz-1;
+// |d| <= 4 <= Nz-1, so one wrap at most
 __device__ __forceinline__ int kper(const Grid& g, int k, int d) {
   const int M = g.Nzm1;
-  int kk = (k - 1 + d) % M;
+  int kk = k - 1 + d;
   if (kk < 0) kk += M;
+  if (kk >= M) kk -= M;
   return kk + 1;
 }
 
@@ -83,11 +89,22 @@ __device__ __forceinline__ double2 ko6(double2 m3, double2 m2, double2 m1, doubl
               p3);
 }
 __device__ __forceinline__ double2 cdiv(double2 a, double s) { return c2(a.x / s, a.y / s); }
+// a / b from the correctly rounded reciprocal rb and one Markstein correction
+// (q = a rb, r = a - q b, q + r rb): the IEEE quotient for dividends above about
+// 2^-1000 in magnitude, at three operations instead of a division sequence
+__device__ __forceinline__ double qdiv(double a, double b, double rb) {
+  const double q = a * rb;
+  const double r = __fma_rn(-q, b, a);
+  return __fma_rn(r, rb, q);
+}
+__device__ __forceinline__ double2 cqdiv(double2 a, double b, double rb) { return c2(qdiv(a.x, b, rb), qdiv(a.y, b, rb)); }
+constexpr double kSixth = 1.0 / 6.0;
 
 // RHS and RK4 combination at one stored point (ii, jj, k).  S(v, i, j) returns
-// variable v of the stage input at (i, j) on plane k, P(v, kk) at the point's
-// own (ii, jj) on plane kk; the two kernels below differ only in where S and P
-// read from, so they produce the same bits.
+// variable v of the stage input at (i, j) on plane k, P(v, d) at the point's
+// own (ii, jj) on the plane d steps away in phi (d = -3..3, d != 0; only asked
+// for 1 <= k <= Nz-1); the two kernels below differ only in where S and P read
+// from, so they produce the same bits.
 template <int KIND, class SF, class PF>
 __device__ __forceinline__ void cfg_point(const CfgArgs& a, int ii, int jj, int k, const SF& S, const PF& P) {
   const Grid& g = a.g;
@@ -107,15 +124,14 @@ __device__ __forceinline__ void cfg_point(const CfgArgs& a, int ii, int jj, int 
     }
   } else {
     const double al = ldm(M.alpha, q), b1 = ldm(M.beta, q), sg = ldm(M.sqrtg, q), dxb = ldm(a.dxb4, q);
-    const int km2 = kper(g, k, -2), km1 = kper(g, k, -1), kp1 = kper(g, k, 1), kp2 = kper(g, k, 2);
     // alpha Pi + beta psi_1 on this plane (ES) and in the own column (EP)
     auto ES = [&](int i2, int j2) {
       const int q2 = off2(g, i2, j2);
       return cadd(rmul(ldm(M.alpha, q2), S(4, i2, j2)), rmul(ldm(M.beta, q2), S(1, i2, j2)));
     };
-    auto EP = [&](int k2) { return cadd(rmul(ldm(M.alpha, q), P(4, k2)), rmul(ldm(M.beta, q), P(1, k2))); };
-    auto Fp = [&](int k2) {
-      return rmul(ldm(M.asg, q), cadd(rmul(ldm(M.grp, q), P(1, k2)), rmul(ldm(M.gpp, q), P(3, k2))));
+    auto EP = [&](int d) { return cadd(rmul(ldm(M.alpha, q), P(4, d)), rmul(ldm(M.beta, q), P(1, d))); };
+    auto Fp = [&](int d) {
+      return rmul(ldm(M.asg, q), cadd(rmul(ldm(M.grp, q), P(1, d)), rmul(ldm(M.gpp, q), P(3, d))));
     };
     // sqrt(gamma) carries the sign of sin(theta) through the pole: negative on the ghost rows
     auto H = [&](int j2) {
@@ -130,7 +146,7 @@ __device__ __forceinline__ void cfg_point(const CfgArgs& a, int ii, int jj, int 
       r[1] = cadd(cadd(d4r(g, fA, ii, a.rr), rmul(b1, d4r(g, fP, ii, a.rr))), rmul(dxb, ps1));
     }
     r[2] = d4c(ES(ii, jj - 2), ES(ii, jj - 1), ES(ii, jj + 1), ES(ii, jj + 2), a.rt);
-    r[3] = d4c(EP(km2), EP(km1), EP(kp1), EP(kp2), a.rp);
+    r[3] = d4c(EP(-2), EP(-1), EP(1), EP(2), a.rp);
     {
       auto fG = [&](int i2) {
         const int q2 = off2(g, i2, jj);
@@ -141,15 +157,15 @@ __device__ __forceinline__ void cfg_point(const CfgArgs& a, int ii, int jj, int 
         const double s2 = ldm(M.sqrtg, off2(g, i2, jj));
         return c2(w.x * s2, w.y * s2);
       };
-      const double2 t1 = cdiv(d4r(g, fG, ii, a.rr), sg);
-      const double2 t2 = cdiv(d4c(H(jj - 2), H(jj - 1), H(jj + 1), H(jj + 2), a.rt), sg);
-      const double2 t3 = cdiv(d4c(Fp(km2), Fp(km1), Fp(kp1), Fp(kp2), a.rp), sg);
+      const double rs = ldm(a.rsg, q);
+      const double2 t1 = cqdiv(d4r(g, fG, ii, a.rr), sg, rs);
+      const double2 t2 = cqdiv(d4c(H(jj - 2), H(jj - 1), H(jj + 1), H(jj + 2), a.rt), sg, rs);
+      const double2 t3 = cqdiv(d4c(Fp(-2), Fp(-1), Fp(1), Fp(2), a.rp), sg, rs);
       const double2 t4 = c2(pi.x * dxb, pi.y * dxb);
-      const double2 t5 = cdiv(rmul(b1, d4r(g, fQ, ii, a.rr)), sg);
+      const double2 t5 = cqdiv(rmul(b1, d4r(g, fQ, ii, a.rr)), sg, rs);
       const double2 t6 = rmul(ldm(M.am2, q), S(0, ii, jj));
       r[4] = csub(cadd(cadd(cadd(cadd(t1, t2), t3), t4), t5), t6);
     }
-    const int km3 = kper(g, k, -3), kp3 = kper(g, k, 3);
     const bool kor = ii >= 3 && ii <= n - 3;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -159,8 +175,7 @@ __device__ __forceinline__ void cfg_point(const CfgArgs& a, int ii, int jj, int 
                                    S(v, ii + 1, jj), S(v, ii + 2, jj), S(v, ii + 3, jj))));
       s = cadd(s, rmul(a.kt, ko6(S(v, ii, jj - 3), S(v, ii, jj - 2), S(v, ii, jj - 1), S(v, ii, jj),
                                  S(v, ii, jj + 1), S(v, ii, jj + 2), S(v, ii, jj + 3))));
-      s = cadd(s, rmul(a.kp, ko6(P(v, km3), P(v, km2), P(v, km1), S(v, ii, jj), P(v, kp1), P(v, kp2),
-                                 P(v, kp3))));
+      s = cadd(s, rmul(a.kp, ko6(P(v, -3), P(v, -2), P(v, -1), S(v, ii, jj), P(v, 1), P(v, 2), P(v, 3))));
       r[v] = s;
     }
   }
@@ -182,7 +197,7 @@ __device__ __forceinline__ void cfg_point(const CfgArgs& a, int ii, int jj, int 
       a.acc[o] = cadd(a.acc[o], rmul(2.0, kk));
       res = cadd(b, kk);
     } else {
-      res = cadd(b, cdivr(cadd(a.acc[o], kk), 6.0));
+      res = cadd(b, cqdiv(cadd(a.acc[o], kk), 6.0, kSixth));
     }
     a.out[o] = res;
   }
@@ -198,7 +213,7 @@ __global__ void __launch_bounds__(128) cfg_stage_kernel(CfgArgs a) {
   if (ii >= g.NI) return;
   const double2* U = a.in;
   auto S = [&](int v, int i2, int j2) { return ldf(U + (long long)v * g.fs, off3(g, i2, j2, k)); };
-  auto P = [&](int v, int k2) { return ldf(U + (long long)v * g.fs, off3(g, ii, jj, k2)); };
+  auto P = [&](int v, int d) { return ldf(U + (long long)v * g.fs, off3(g, ii, jj, kper(g, k, d))); };
   cfg_point<KIND>(a, ii, jj, k, S, P);
 }
 
@@ -209,7 +224,9 @@ __global__ void __launch_bounds__(128) cfg_stage_kernel(CfgArgs a) {
 // buffered: the next plane's tile is copied by cp.async while this plane is
 // computed.  The phi neighbours of the thread's own column (planes k+-1..3)
 // are read through the read-only cache; the same values serve seven
-// consecutive planes of the march.
+// consecutive planes of the march.  (Holding them in a rolling register window
+// instead needs 255 registers per thread and one CTA per SM, and ran the C0
+// grid at half the speed.)
 constexpr int CTI = 32, CTJ = 8, CRH = 4, CTH = 3;
 constexpr int CW = CTI + 2 * CRH, CH = CTJ + 2 * CTH, CT_N = CW * CH;
 constexpr size_t CFG_TILE_BYTES = (size_t)5 * CT_N * sizeof(double2);
@@ -252,7 +269,7 @@ __global__ void __launch_bounds__(CTI * CTJ, 2) cfg_march_kernel(CfgArgs a, int 
       // every same-plane neighbour lies inside the halo tile
       const double2* T = tiles + (size_t)buf * 5 * CT_N + (ty + CTH) * CW + (tx + CRH);
       auto S = [&](int v, int i2, int j2) { return T[v * CT_N + (j2 - jj) * CW + (i2 - ii)]; };
-      auto P = [&](int v, int k2) { return ldf(col + (long long)v * g.fs, (long long)k2 * g.plane); };
+      auto P = [&](int v, int d) { return ldf(col + (long long)v * g.fs, (long long)kper(g, k, d) * g.plane); };
       cfg_point<KIND>(a, ii, jj, k, S, P);
     }
     __syncthreads();
@@ -321,12 +338,13 @@ int cfg_march_launch(const CfgArgs& a, cudaStream_t st) {
 
 }  // namespace
 
-int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, const double coef[6], double rN,
-                     int tiled, cudaStream_t st) {
+int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, const double* rsg, const double coef[6],
+                     double rN, int tiled, cudaStream_t st) {
   CfgArgs a;
   a.g = L.g;
   a.m = L.m;
   a.dxb4 = dxbeta4;
+  a.rsg = rsg;
   a.in = L.in[0];
   a.base = L.base;
   a.acc = L.acc;

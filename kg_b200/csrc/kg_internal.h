@@ -89,10 +89,11 @@ void launch_ghost_fill_f32(const void* d_desc, int n, long long max_rows, long l
                            cudaStream_t st);
 // configured method (kg_config.cu): RK4 stage with fourth-order differences,
 // Kreiss-Oliger dissipation and a Sommerfeld outer plane; coef = 1/(12 h) for
-// r, theta, phi then eps/(64 h) for r, theta, phi; rN = outermost r; tiled = 1
-// for the shared-memory tiled marching form, 0 for one thread per point (same bits)
-int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, const double coef[6], double rN,
-                     int tiled, cudaStream_t st);
+// r, theta, phi then eps/(64 h) for r, theta, phi; rN = outermost r; rsg = the
+// 1/sqrt(gamma) table; tiled = 1 for the shared-memory tiled marching form, 0 for
+// one thread per point (same bits)
+int launch_stage_cfg(int kind, const StageLaunch& L, const double* dxbeta4, const double* rsg, const double coef[6],
+                     double rN, int tiled, cudaStream_t st);
 void launch_ghost_fill_cfg(const Grid& g, double2* u, cudaStream_t st);
 // Berger-Oliger transfers between radially nested 2:1 levels (kg_refine.cu)
 // uf_pi: where the fine Pi variable lives (nullptr: uf + 4 fs, the 5-variable layout)
