@@ -36,6 +36,10 @@ using namespace tmaops;
 namespace {
 
 constexpr int TI = 32, TJ = 8, RH = 2;
+template <bool B>
+struct TBool {
+  static constexpr bool value = B;
+};
 constexpr int RW = 2 * (TI + 2 * RH);         // ring row width in doubles (72 = 576 B)
 constexpr int RROWS = TJ + 2;                 // theta rows with halo
 constexpr int FIELD_D = RROWS * RW;           // doubles per variable per plane
@@ -204,6 +208,12 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
   bool failed = __syncthreads_or(timed_out) != 0;
   const int last = k1 - k0 - 1;
 
+  // FAST: every lane of the warp is two points inside the array in r and beta^r > 0
+  // there, so every lane takes the centred derivative and the forward upwind
+  // difference (the branches the general form would take); warp-uniform
+  const bool fast = __all_sync(0xffffffffu, act && ii >= 2 && ii <= g.NI - 3 && be > 0.0);
+  auto march = [&](auto fastc) {
+  constexpr bool FAST = decltype(fastc)::value;
   for (int i = 0; i <= last && !failed; ++i) {
     const int k = k0 + i;
     if (tid == 0 && !timed_out) {
@@ -246,12 +256,14 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
           auto aPi = [&](int dx) { return rmul(MTV(MT_AL, tx + dx, ty), RF(cu, 4, tx + dx, ty)); };
           auto ps1 = [&](int dx) { return RF(cu, 1, tx + dx, ty); };
           double2 d;
-          if (ii == 0) d = fwd3(aPi(0), aPi(1), aPi(2));
+          if (FAST) d = ctr(aPi(-1), aPi(1));
+          else if (ii == 0) d = fwd3(aPi(0), aPi(1), aPi(2));
           else if (ii == n) d = bwd3(aPi(0), aPi(-1), aPi(-2));
           else d = ctr(aPi(-1), aPi(1));
           d = rmul(g.rdx, d);
           double2 av;
-          if (ii <= 1) av = fwd3(fcu[1], ps1(1), ps1(2));
+          if (FAST) av = fwd3(fcu[1], ps1(1), ps1(2));
+          else if (ii <= 1) av = fwd3(fcu[1], ps1(1), ps1(2));
           else if (ii == n - 1) av = csub(ps1(1), ps1(-1));
           else if (ii == n) av = bwd3(fcu[1], ps1(-1), ps1(-2));
           else if (be > 0.0) av = fwd3(fcu[1], ps1(1), ps1(2));
@@ -287,7 +299,8 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
             return rmul(MTV(MT_A, tx + dx, ty), RF(cu, 1, tx + dx, ty));
           };
           double2 d;
-          if (ii == 0) d = fwd3(G1(0), G1(1), G1(2));
+          if (FAST) d = ctr(G1(-1), G1(1));
+          else if (ii == 0) d = fwd3(G1(0), G1(1), G1(2));
           else if (ii == n) d = bwd3(G1(0), G1(-1), G1(-2));
           else d = ctr(G1(-1), G1(1));
           const double2 r1 = cdivm(rmul(g.rdx, d), sg, rs);
@@ -309,7 +322,8 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
           const double2 r4 = rmul(dxb, fcu[4]);
           auto Q = [&](int dx) { return rmul(MTV(MT_SG, tx + dx, ty), RF(cu, 4, tx + dx, ty)); };
           double2 av;
-          if (ii <= 1) av = fwd3(Q(0), Q(1), Q(2));
+          if (FAST) av = fwd3(Q(0), Q(1), Q(2));
+          else if (ii <= 1) av = fwd3(Q(0), Q(1), Q(2));
           else if (ii == n - 1) av = csub(Q(1), Q(-1));
           else if (ii == n) av = bwd3(Q(0), Q(-1), Q(-2));
           else if (be > 0.0) av = fwd3(Q(0), Q(1), Q(2));
@@ -378,6 +392,9 @@ __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtenso
     release(i + 1);
     if (i == last) release(i + 2);
   }
+  };
+  if (fast) march(TBool<true>());
+  else march(TBool<false>());
   failed = __syncthreads_or(timed_out) != 0;
   if (failed) {
     if (tid == 0) {
