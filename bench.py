@@ -296,10 +296,12 @@ def engine_leg(reqs, device, tune, steps=10):
 def _tdesc(t):
     """a Tuning as the bench line reports it"""
     if t.dispatch == 1:
-        form = {0: "one thread per point", 1: "32x8 tiles, register prefetch", 2: "32x8 tiles, TMA ring"}
+        form = {0: "one thread per point", 1: "32x8 tiles, register prefetch",
+                2: f"32x{t.tile_rows} tiles, TMA ring"}
         return {"dispatch": "concurrent single-solve launches, one stream per solve",
                 "stage_kernel_form": form.get(t.variant, t.variant)}
-    return {"dispatch": "persistent launch per stage over all solves", "kchunk": t.kchunk, "ctas": t.blocks}
+    return {"dispatch": "persistent launch per stage over all solves", "kchunk": t.kchunk, "ctas": t.blocks,
+            "tile": f"32x{t.tile_rows}"}
 
 
 def _wave(d):

@@ -230,6 +230,12 @@ long long kg_launch_count(const kg_solver *h);
  * (kg_set_scheme) takes 0 for one thread per point and any other value for
  * its tiled form, which gives the same bits. */
 int kg_set_kernel_variant(kg_solver *h, int variant);
+/* theta rows of the TMA tiles of the RK4 stages (FP64 forms 2, 3 and the mixed
+ * form): 8 (default; 32 x 8 tiles, 2 CTAs per SM) or 4 (32 x 4 tiles, 3 CTAs per
+ * SM, twice the tiles per grid).  The same bits either way.  No reference
+ * counterpart. */
+int kg_set_tile_rows(kg_solver *h, int rows);
+int kg_get_tile_rows(const kg_solver *h);
 
 /* --- batched engine ------------------------------------------------------------ */
 /* No reference counterpart (the reference runs one solve per MPI job): many
@@ -266,10 +272,15 @@ int kg_batch_get_tuning(const kg_batch *b, int *kchunk, int *blocks);
  * on its own stream, all members concurrently, forked from and joined back into
  * the batch stream (the same bits as kg_rk4 on each member alone).  variant: in
  * dispatch 1 the members' stage-kernel form (kg_set_kernel_variant), -1 to keep
- * each member's own; the mixed form takes -1 or 2..5.  The tuner's third and
+ * each member's own; the mixed form takes -1, 2 or 3.  The tuner's third and
  * fourth knobs. */
 int kg_batch_set_dispatch(kg_batch *b, int dispatch, int variant);
 int kg_batch_get_dispatch(const kg_batch *b, int *dispatch, int *variant);
+/* theta rows of the TMA tiles (8 or 4, as kg_set_tile_rows): the persistent
+ * launch's work items, and in dispatch 1 every member's RK4 stage kernels.  The
+ * tuner's fifth knob. */
+int kg_batch_set_tile_rows(kg_batch *b, int rows);
+int kg_batch_get_tile_rows(const kg_batch *b, int *rows);
 long long kg_batch_launch_count(const kg_batch *b);
 void *kg_batch_get_stream(const kg_batch *b);
 

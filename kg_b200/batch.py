@@ -92,15 +92,17 @@ class Batch:
             off += a * b * c
         return res
 
-    def set_tuning(self, kchunk, blocks, dispatch=0, variant=-1):
+    def set_tuning(self, kchunk, blocks, dispatch=0, variant=-1, tile_rows=8):
         self._ck(self._lib.kg_batch_set_tuning(self._b, int(kchunk), int(blocks)))
         self._ck(self._lib.kg_batch_set_dispatch(self._b, int(dispatch), int(variant)))
+        self._ck(self._lib.kg_batch_set_tile_rows(self._b, int(tile_rows)))
 
     def tuning(self):
-        k, b, d, v = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+        k, b, d, v, r = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
         self._ck(self._lib.kg_batch_get_tuning(self._b, C.byref(k), C.byref(b)))
         self._ck(self._lib.kg_batch_get_dispatch(self._b, C.byref(d), C.byref(v)))
-        return Tuning(k.value, b.value, d.value, v.value)
+        self._ck(self._lib.kg_batch_get_tile_rows(self._b, C.byref(r)))
+        return Tuning(k.value, b.value, d.value, v.value, r.value)
 
     @property
     def launch_count(self):
@@ -112,32 +114,40 @@ class Batch:
 
 
 class Tuning(tuple):
-    """(kchunk, blocks, dispatch, variant): the arguments of Batch.set_tuning"""
+    """(kchunk, blocks, dispatch, variant, tile_rows): the arguments of Batch.set_tuning"""
 
-    def __new__(cls, kchunk, blocks, dispatch=0, variant=-1):
-        return super().__new__(cls, (int(kchunk), int(blocks), int(dispatch), int(variant)))
+    def __new__(cls, kchunk, blocks, dispatch=0, variant=-1, tile_rows=8):
+        return super().__new__(cls, (int(kchunk), int(blocks), int(dispatch), int(variant), int(tile_rows)))
 
     kchunk = property(lambda self: self[0])
     blocks = property(lambda self: self[1])
     dispatch = property(lambda self: self[2])
     variant = property(lambda self: self[3])
+    tile_rows = property(lambda self: self[4])
 
 
 _TUNE_CACHE = {}
 
 
 def candidates(precision="fp64", kchunks=(16, 24, 32, 48, 64), ctas_per_sm=(1, 2), sms=148,
-               variants=(2, 1, 0)):
-    """The tuner's search space: persistent launches over (kchunk, CTAs per SM),
-    and concurrent single-solve launches over the stage-kernel forms (the mixed
-    form has the TMA form only)."""
-    out = [Tuning(kc, cps * sms, 0, -1) for kc in kchunks for cps in ctas_per_sm]
-    out += [Tuning(kchunks[0], sms, 1, v) for v in (variants if precision == "fp64" else (2,))]
+               variants=(2, 1, 0), tile_rows=(8, 4)):
+    """The tuner's search space: persistent launches over (kchunk, CTAs per SM,
+    tile rows), and concurrent single-solve launches over the stage-kernel forms
+    (the mixed form has the TMA form only), the TMA form in each tile height.
+    A 32 x 4 tile holds half the threads and shared memory of a 32 x 8 one, so its
+    persistent launches run 1.5x the CTAs per SM."""
+    out = []
+    for tr in tile_rows:
+        per_sm = ctas_per_sm if tr == 8 else tuple(sorted({max(1, (3 * c) // 2) for c in ctas_per_sm}))
+        out += [Tuning(kc, cps * sms, 0, -1, tr) for kc in kchunks for cps in per_sm]
+    for v in (variants if precision == "fp64" else (2,)):
+        for tr in (tile_rows if v == 2 else (8,)):
+            out.append(Tuning(kchunks[0], sms, 1, v, tr))
     return out
 
 
 def autotune(shapes, device=-1, kchunks=(16, 24, 32, 48, 64), ctas_per_sm=(1, 2), steps=3, sms=None,
-             precision="fp64", variants=(2, 1, 0)):
+             precision="fp64", variants=(2, 1, 0), tile_rows=(8, 4)):
     """Choose how a batch of solves with the given grid shapes runs (a Tuning).
 
     shapes: list of (Nx, Ny, Nz).  Every candidate of `candidates` is timed on
@@ -155,7 +165,7 @@ def autotune(shapes, device=-1, kchunks=(16, 24, 32, 48, 64), ctas_per_sm=(1, 2)
     scratch = [ScalarField(nx, ny, nz, 1.8, 1.8 + 0.1 * nx, 0.25, device=device, n_det=2, l_max=0)
                for (nx, ny, nz) in shapes]
     best = None
-    for cand in candidates(precision, kchunks, ctas_per_sm, sms, variants):
+    for cand in candidates(precision, kchunks, ctas_per_sm, sms, variants, tile_rows):
         b = Batch(device, precision=precision)
         for s in scratch:
             b.add(s)

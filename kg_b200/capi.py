@@ -89,6 +89,8 @@ SIGNATURES = [
     ("kg_profile_kind_name", C.c_char_p, [_I]),
     ("kg_launch_count", C.c_longlong, [_P]),
     ("kg_set_kernel_variant", _I, [_P, _I]),
+    ("kg_set_tile_rows", _I, [_P, _I]),
+    ("kg_get_tile_rows", _I, [_P]),
     ("kg_batch_create", _I, [_I, _PP]),
     ("kg_batch_destroy", _I, [_P]),
     ("kg_batch_last_error", C.c_char_p, [_P]),
@@ -116,6 +118,8 @@ SIGNATURES = [
     ("kg_batch_get_tuning", _I, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("kg_batch_set_dispatch", _I, [_P, _I, _I]),
     ("kg_batch_get_dispatch", _I, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("kg_batch_set_tile_rows", _I, [_P, _I]),
+    ("kg_batch_get_tile_rows", _I, [_P, C.POINTER(C.c_int)]),
     ("kg_batch_launch_count", C.c_longlong, [_P]),
     ("kg_batch_get_stream", C.c_void_p, [_P]),
     ("kg_integrate_mass_noalloc", _I, [C.c_void_p, C.c_void_p, _I, _I, _I, C.c_double, C.c_double,

@@ -65,7 +65,8 @@ struct kg_solver {
   double* partials = nullptr;            // mass partial sums + result
   int s_cur = 4, t_cur = 4;              // slot holding the current Pi stage value
   int variant = 3;                       // 0: per-point, 1: 2.5-D marching, 2, 3: TMA-pipelined marching
-                                         // (3, 4, 5: PIRK stage 1 fused in one kernel; 2: two launches)
+                                         // (3: PIRK stage 1 fused in one kernel; 2: two launches)
+  int tile_rows = 8;                     // theta rows of the TMA tiles of the RK4 stages (8 or 4)
   int* derr = nullptr;                   // device flag: a bounded wait in a kernel ran out
   // CUDA graphs of two consecutive steps per stepper and Pi-slot state
   int use_graphs = 1;
@@ -714,7 +715,7 @@ int store_view(kg_solver* h, const View& V, double* dst, cudaMemcpyKind kind) {
 void run_stage(kg_solver* h, int kind, const kg::StageLaunch& L) {
   Prof pf(h, kind, 1);
   const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
-  if (h->variant >= 2 && kg::launch_stage_tma(kind, L, rsg, h->derr, h->stream) == 0) return;
+  if (h->variant >= 2 && kg::launch_stage_tma(kind, L, rsg, h->derr, h->stream, h->tile_rows) == 0) return;
   if (h->variant >= 1)
     kg::launch_stage_march(kind, L, rsg, h->stream);
   else
@@ -1077,7 +1078,7 @@ int run_mixed_stage(kg_solver* h, int st, const kg::MixedLaunch& L) {
   static const int kinds[4] = {kg::ST_RK4_1, kg::ST_RK4_2, kg::ST_RK4_3, kg::ST_RK4_4};
   Prof pf(h, PK_MX1 + st, 1);
   const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
-  if (kg::launch_stage_mixed(kinds[st], L, rsg, h->derr, h->stream))
+  if (kg::launch_stage_mixed(kinds[st], L, rsg, h->derr, h->stream, h->tile_rows))
     return set_err(h, KG_ECUDA, "mixed-precision stage could not be configured (tensor maps)");
   return KG_OK;
 }
@@ -1935,6 +1936,17 @@ int kg_set_kernel_variant(kg_solver* h, int variant) {
   return KG_OK;
 }
 
+int kg_set_tile_rows(kg_solver* h, int rows) {
+  if (!h || (rows != 4 && rows != 8)) return KG_EINVAL;
+  if (rows != h->tile_rows) {
+    h->tile_rows = rows;
+    h->graph_gen++;
+  }
+  return KG_OK;
+}
+
+int kg_get_tile_rows(const kg_solver* h) { return h ? h->tile_rows : KG_EINVAL; }
+
 int kg_profile_enable(kg_solver* h, int on) {
   if (!h) return KG_EINVAL;
   h->prof_on = on ? 1 : 0;
@@ -2002,6 +2014,9 @@ struct kg_batch {
   // in dispatch 1 (-1 keeps each member's own)
   int dispatch = 0;
   int variant = -1;
+  // theta rows of the TMA tiles (8 or 4): the persistent launch's work items,
+  // and in dispatch 1 every member's RK4 stage kernels
+  int tile_rows = 8;
 };
 
 #define KG_BCK(call)                                                        \
@@ -2065,7 +2080,7 @@ int batch_rebuild(kg_batch* b) {
         M.skip_last_i = st == 3 ? inflow : 0;
         const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
         const int ni = kg::build_mixed_item(hitems.data() + (size_t)i * isz, kinds[st], M, rsg, b->derr, b->kchunk,
-                                            item0);
+                                            item0, b->tile_rows);
         if (ni < 0) {
           b->err = "tensor-map encoding failed for a batch member";
           return KG_ECUDA;
@@ -2096,7 +2111,7 @@ int batch_rebuild(kg_batch* b) {
       L.skip_last_i = (st == 3) ? (h->p.bc_rmax == KG_INFLOW) : 0;
       const double* rsg = h->dmet + (size_t)T_RSG * h->NJ * h->PI;
       const int ni = kg::build_batch_item(hitems.data() + (size_t)i * isz, kinds[st], L, rsg, b->derr, b->kchunk,
-                                          item0);
+                                          item0, b->tile_rows);
       if (ni < 0) {
         b->err = "tensor-map encoding failed for a batch member";
         return KG_ECUDA;
@@ -2130,9 +2145,9 @@ int batch_enqueue_step(kg_batch* b) {
   for (int st = 0; st < 4; ++st) {
     const int bad = b->precision == 1
                         ? kg::launch_batch_mixed(kinds[st], b->metric_kind, b->ditems[st], n, b->n_items[st],
-                                                 b->blocks, b->stream)
+                                                 b->blocks, b->tile_rows, b->stream)
                         : kg::launch_batch_tma(kinds[st], b->metric_kind, b->ditems[st], n, b->n_items[st],
-                                               b->blocks, b->stream);
+                                               b->blocks, b->tile_rows, b->stream);
     if (bad) {
       b->err = "batched stage launch could not be configured";
       return KG_ECUDA;
@@ -2246,6 +2261,10 @@ int kg_batch_rk4(kg_batch* b, int nsteps) {
     for (kg_solver* h : b->members) {
       if (b->variant >= 0 && h->variant != b->variant) {
         h->variant = b->variant;
+        h->graph_gen++;
+      }
+      if (h->tile_rows != b->tile_rows) {
+        h->tile_rows = b->tile_rows;
         h->graph_gen++;
       }
       rc = b->precision ? run_steps(h, 4, nsteps, step_rk4_mixed) : run_steps(h, 3, nsteps, step_rk4);
@@ -2404,6 +2423,21 @@ int kg_batch_set_dispatch(kg_batch* b, int dispatch, int variant) {
   }
   b->dispatch = dispatch;
   b->variant = variant;
+  return KG_OK;
+}
+
+int kg_batch_set_tile_rows(kg_batch* b, int rows) {
+  if (!b || (rows != 4 && rows != 8)) return KG_EINVAL;
+  if (rows != b->tile_rows) {
+    b->tile_rows = rows;
+    b->dirty = true;  // the work items and their tensor maps depend on the tile
+  }
+  return KG_OK;
+}
+
+int kg_batch_get_tile_rows(const kg_batch* b, int* rows) {
+  if (!b || !rows) return KG_EINVAL;
+  *rows = b->tile_rows;
   return KG_OK;
 }
 

@@ -39,9 +39,10 @@ struct StageLaunch {
 void launch_stage(int kind, const StageLaunch& L, cudaStream_t st);
 // 2.5-D marching form of the same kernels (kg_march.cu); rsg = 1/sqrt(gamma) table
 void launch_stage_march(int kind, const StageLaunch& L, const double* rsg, cudaStream_t st);
-// TMA-pipelined form (kg_tma.cu); err: device flag set to 1 when a bounded wait runs out.
+// TMA-pipelined form (kg_tma.cu); err: device flag set to 1 when a bounded wait runs out;
+// tj: theta rows of a tile, 8, or 4 for the RK4 stages (other kinds run 8).
 // Returns 0, or -1 if the tensor maps cannot be encoded / the kernel cannot be configured.
-int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st);
+int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st, int tj = 8);
 // PIRK stage 1 in one kernel (kg_fused.cu): S(1:4) = u + dt rhs(u), Snew = u(5) +
 // dt rhs_pi(S(1:4), Sold).  Returns -1 if the tensor maps cannot be encoded.
 int launch_pirk_s1_fused(const Grid& g, const Metric& m, int mk, const double2* U, const double2* Sold, double2* S,
@@ -50,8 +51,10 @@ int launch_pirk_s1_fused(const Grid& g, const Metric& m, int mk, const double2* 
 bool tma_available(const Grid& g, const double2* some_state);
 // batched (multi-solve) persistent launches of the TMA stage kernel
 size_t batch_item_bytes();
-int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rsg, int* err, int kchunk, int item0);
-int launch_batch_tma(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks, cudaStream_t st);
+int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rsg, int* err, int kchunk, int item0,
+                     int tj);
+int launch_batch_tma(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks, int tj,
+                     cudaStream_t st);
 // Y_lm projection over all shells (kg_ylm_gemm.cu)
 int ylm_gemm_pad_m(int rows);
 int ylm_gemm_pad_n(int cols);
@@ -78,10 +81,12 @@ struct MixedLaunch {
   double2* out_d;        // u^{n+1} (stage 4)
   int skip_last_i;
 };
-int launch_stage_mixed(int kind, const MixedLaunch& L, const double* rsg, int* err, cudaStream_t st);
+// tj: theta rows of a tile, 8 or 4 (other values: 8 for a single solve, an error for a batch)
+int launch_stage_mixed(int kind, const MixedLaunch& L, const double* rsg, int* err, cudaStream_t st, int tj = 8);
 size_t mixed_item_bytes();
-int build_mixed_item(void* dst, int kind, const MixedLaunch& L, const double* rsg, int* err, int kchunk, int item0);
-int launch_batch_mixed(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks,
+int build_mixed_item(void* dst, int kind, const MixedLaunch& L, const double* rsg, int* err, int kchunk, int item0,
+                     int tj);
+int launch_batch_mixed(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks, int tj,
                        cudaStream_t st);
 size_t ghost_f32_desc_bytes();
 void fill_ghost_f32_desc(void* dst, const Grid& g, float2* u, const double2* up, int inflow);

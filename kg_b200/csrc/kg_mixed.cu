@@ -32,29 +32,36 @@ namespace kg {
 using namespace tmaops;
 namespace {
 
-constexpr int TI = 32, TJ = 8, RH = 2;
+constexpr int TI = 32, RH = 2;
 constexpr int RW = 2 * (TI + 2 * RH);  // ring row width in elements (two per complex value)
-constexpr int RROWS = TJ + 2;
-constexpr int FIELD_E = RROWS * RW;
-constexpr int STAGE_E = 5 * FIELD_E;
 constexpr int NST = 3;
-// ring slot stride in elements: TMA destinations start on 128-byte boundaries
-template <class T>
-__host__ __device__ constexpr int slot_e() {
-  return (int)(((STAGE_E * sizeof(T) + 127) / 128) * 128 / sizeof(T));
-}
-constexpr int MW = TI + 2 * RH, MH = TJ + 2, MT_N = MW * MH;
+constexpr int MW = TI + 2 * RH;
 enum { MT_AL = 0, MT_BE, MT_A, MT_GRR, MT_GRP, MT_SG, MT_HT, MT_COUNT };
-// stages 2-4 (FP32 ring) stage their point-wise operands -- u^n (FP64) and the
-// increment sum (FP32), five variables of the thread's own point -- in shared
-// memory with cp.async issued at the start of each plane, so the loads run
-// under the RHS arithmetic instead of after it
-constexpr int STG_BYTES = TI * TJ * 5 * (16 + 8);
-template <class T>
-__host__ __device__ constexpr size_t mx_smem() {
-  return (size_t)NST * slot_e<T>() * sizeof(T) + (size_t)MT_COUNT * MT_N * 8 + 64 + 128 +
-         (sizeof(T) == 4 ? (size_t)STG_BYTES + (size_t)MT_COUNT * MT_N * 4 : 0);
-}
+// tile geometry for TJ theta rows (one warp per row): 8 (256 threads, 2 CTAs
+// per SM) or 4 (128 threads, 3 CTAs per SM)
+template <int TJ>
+struct MGeom {
+  static constexpr int RROWS = TJ + 2;
+  static constexpr int FIELD_E = RROWS * RW;
+  static constexpr int STAGE_E = 5 * FIELD_E;
+  static constexpr int MH = TJ + 2, MT_N = MW * MH;
+  // stages 2-4 (FP32 ring) stage their point-wise operands -- u^n (FP64) and the
+  // increment sum (FP32), five variables of the thread's own point -- in shared
+  // memory with cp.async issued at the start of each plane, so the loads run
+  // under the RHS arithmetic instead of after it
+  static constexpr int STG_BYTES = TI * TJ * 5 * (16 + 8);
+  static constexpr int MIN_BLOCKS = TJ == 4 ? 3 : 2;
+  // ring slot stride in elements: TMA destinations start on 128-byte boundaries
+  template <class T>
+  static __host__ __device__ constexpr int slot_e() {
+    return (int)(((STAGE_E * sizeof(T) + 127) / 128) * 128 / sizeof(T));
+  }
+  template <class T>
+  static __host__ __device__ constexpr size_t smem() {
+    return (size_t)NST * slot_e<T>() * sizeof(T) + (size_t)MT_COUNT * MT_N * 8 + 64 + 128 +
+           (sizeof(T) == 4 ? (size_t)STG_BYTES + (size_t)MT_COUNT * MT_N * 4 : 0);
+  }
+};
 
 // ---- a complex value in arithmetic type R -----------------------------------
 template <class R>
@@ -129,10 +136,11 @@ namespace {
 
 // RHS of all five variables at the thread's own point, arithmetic in R.
 // cu: ring slot of plane k; E/F: phi-derivative arguments at k-1 and k+1.
-template <class R, int MK, class TIN>
+template <class R, int MK, class TIN, int TJ>
 __device__ __forceinline__ void mx_rhs(const MxArgs& a, const TIN* cu, const double* mt, const float* mtf, int tx,
                                        int ty, int ii, int jj, int k, const double* own, double2 Epv, double2 Enx,
                                        double2 Fpv, double2 Fnx, cx<R> r[5]) {
+  constexpr int FIELD_E = MGeom<TJ>::FIELD_E, MT_N = MGeom<TJ>::MT_N;
   const Grid& g = a.g;
   const Metric& M = a.m;
   const TIN* gin = reinterpret_cast<const TIN*>(a.in);
@@ -242,8 +250,9 @@ __device__ __forceinline__ void mx_rhs(const MxArgs& a, const TIN* cu, const dou
 }
 
 // phi-derivative arguments at the own point of a ring slot, in R, widened
-template <class R, int MK, class TIN>
+template <class R, int MK, class TIN, int TJ>
 __device__ __forceinline__ void mx_EF(const TIN* st, int tx, int ty, const double* own, double2& E, double2& F) {
+  constexpr int FIELD_E = MGeom<TJ>::FIELD_E;
   auto RF = [&](int f) -> cx<R> { return ld2<R>(st + (size_t)f * FIELD_E + (ty + 1) * RW + 2 * (tx + RH)); };
   const R al = (R)own[0], be = (R)own[1], fa = (R)own[6], fgrp = (R)own[7], fgpp = (R)own[8];
   const cx<R> e = add(sm(al, RF(4)), sm(be, RF(1)));
@@ -254,10 +263,12 @@ __device__ __forceinline__ void mx_EF(const TIN* st, int tx, int ty, const doubl
   F = make_double2((double)f.x, (double)f.y);
 }
 
-template <int KIND, int MK, class TIN>
+template <int KIND, int MK, class TIN, int TJ>
 __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMap* tp0p, const CUtensorMap* tp1p,
                                        const MxArgs& a, int bx, int by, int bz, TIN* ring, double* mt,
                                        uint64_t* bars, uint32_t tb, unsigned char* stg) {
+  using GT = MGeom<TJ>;
+  constexpr int FIELD_E = GT::FIELD_E, STAGE_E = GT::STAGE_E, MT_N = GT::MT_N;
   constexpr bool STG = sizeof(TIN) == 4;
   double2* base_s = reinterpret_cast<double2*>(stg);
   float2* acc_s = reinterpret_cast<float2*>(stg + (size_t)TI * TJ * 5 * 16);
@@ -293,7 +304,8 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
   auto issue = [&](int t) {
     const int s = slot(t);
     mbar_expect_tx(&bars[s], (uint32_t)(STAGE_E * sizeof(TIN)));
-    tma_load_4d(ring + (size_t)s * slot_e<TIN>(), tinp, 2 * (ii0 - RH), jj0 - 1, plane_of(t), 0, &bars[s]);
+    tma_load_4d(ring + (size_t)s * GT::template slot_e<TIN>(), tinp, 2 * (ii0 - RH), jj0 - 1, plane_of(t), 0,
+                &bars[s]);
   };
   // the first planes are requested before the metric tile is loaded, so the
   // copies are in flight while the tile loads (the ring is free: every warp
@@ -349,14 +361,14 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
   // FP64 RHS at the excision side and next to the poles
   const bool hp = (ii <= 1) || (jj <= 1) || (jj >= g.NJ - 2);
   auto EF = [&](const TIN* st, double2& E, double2& F) {
-    if (hp) mx_EF<double, MK, TIN>(st, tx, ty, own, E, F);
-    else mx_EF<float, MK, TIN>(st, tx, ty, own, E, F);
+    if (hp) mx_EF<double, MK, TIN, TJ>(st, tx, ty, own, E, F);
+    else mx_EF<float, MK, TIN, TJ>(st, tx, ty, own, E, F);
   };
   const long long pcol = act ? off3(g, ii, jj, 0) : 0;
   int timed_out = 0;
   double2 Epv = make_double2(0, 0), Fpv = Epv, Ecu = Epv, Fcu = Epv;
   if (!mbar_wait_bounded(&bars[slot(0)], parity(0))) timed_out = 1;
-  if (act && !timed_out) EF(ring + (size_t)slot(0) * slot_e<TIN>(), Epv, Fpv);
+  if (act && !timed_out) EF(ring + (size_t)slot(0) * GT::template slot_e<TIN>(), Epv, Fpv);
   release(0);
   bool failed = __syncthreads_or(timed_out) != 0;
   const int last = k1 - k0 - 1;
@@ -391,20 +403,20 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
       if (!okn) timed_out = 1;
     }
     if (act && !timed_out) {
-      const TIN* cu = ring + (size_t)slot(tc) * slot_e<TIN>();
-      const TIN* nx = ring + (size_t)slot(tn) * slot_e<TIN>();
+      const TIN* cu = ring + (size_t)slot(tc) * GT::template slot_e<TIN>();
+      const TIN* nx = ring + (size_t)slot(tn) * GT::template slot_e<TIN>();
       if (i == 0) EF(cu, Ecu, Fcu);
       double2 Enx, Fnx;
       EF(nx, Enx, Fnx);
       double2 rr[5];
       if (hp) {
         cx<double> r[5];
-        mx_rhs<double, MK, TIN>(a, cu, mt, mtf, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
+        mx_rhs<double, MK, TIN, TJ>(a, cu, mt, mtf, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
 #pragma unroll
         for (int v = 0; v < 5; ++v) rr[v] = make_double2(r[v].x, r[v].y);
       } else {
         cx<float> r[5];
-        mx_rhs<float, MK, TIN>(a, cu, mt, mtf, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
+        mx_rhs<float, MK, TIN, TJ>(a, cu, mt, mtf, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
 #pragma unroll
         for (int v = 0; v < 5; ++v) rr[v] = make_double2((double)r[v].x, (double)r[v].y);
       }
@@ -473,10 +485,11 @@ __device__ __forceinline__ unsigned char* align128(unsigned char* p) {
   return p + ((128u - (a & 127u)) & 127u);
 }
 
+template <int TJ>
 __device__ __forceinline__ void init_bars(uint64_t* bars) {
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
-    for (int s = 0; s < NST; ++s) mbar_init(&bars[NST + s], TI * TJ / 32);
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[NST + s], TJ);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -484,33 +497,37 @@ __device__ __forceinline__ void init_bars(uint64_t* bars) {
 
 }  // namespace
 
-template <int KIND, int MK, class TIN>
-__global__ void __launch_bounds__(TI * TJ, 2)
+template <int KIND, int MK, class TIN, int TJ>
+__global__ void __launch_bounds__(TI * TJ, MGeom<TJ>::MIN_BLOCKS)
     mx_stage_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tp0,
                     const __grid_constant__ CUtensorMap tp1, MxArgs a) {
+  using GT = MGeom<TJ>;
+  constexpr int MT_N = GT::MT_N;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TIN* ring = reinterpret_cast<TIN*>(align128(smem_raw));
-  double* mt = reinterpret_cast<double*>(ring + (size_t)NST * slot_e<TIN>());
+  double* mt = reinterpret_cast<double*>(ring + (size_t)NST * GT::template slot_e<TIN>());
   uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(mt + (size_t)MT_COUNT * MT_N) +
                                                (sizeof(TIN) == 4 ? (size_t)MT_COUNT * MT_N * 4 : 0));
   unsigned char* stg = reinterpret_cast<unsigned char*>(bars + 8);
   if ((int)blockIdx.z * a.kchunk >= a.g.NK) return;
-  init_bars(bars);
-  (void)mx_item<KIND, MK, TIN>(&tin, &tp0, &tp1, a, blockIdx.x, blockIdx.y, blockIdx.z, ring, mt, bars, 0u, stg);
+  init_bars<TJ>(bars);
+  (void)mx_item<KIND, MK, TIN, TJ>(&tin, &tp0, &tp1, a, blockIdx.x, blockIdx.y, blockIdx.z, ring, mt, bars, 0u, stg);
 }
 
-template <int KIND, int MK, class TIN>
-__global__ void __launch_bounds__(TI * TJ, 2) mx_batch_kernel(const MxItem* __restrict__ solves, int n_solves,
-                                                                int n_items) {
+template <int KIND, int MK, class TIN, int TJ>
+__global__ void __launch_bounds__(TI * TJ, MGeom<TJ>::MIN_BLOCKS)
+    mx_batch_kernel(const MxItem* __restrict__ solves, int n_solves, int n_items) {
+  using GT = MGeom<TJ>;
+  constexpr int MT_N = GT::MT_N;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TIN* ring = reinterpret_cast<TIN*>(align128(smem_raw));
-  double* mt = reinterpret_cast<double*>(ring + (size_t)NST * slot_e<TIN>());
+  double* mt = reinterpret_cast<double*>(ring + (size_t)NST * GT::template slot_e<TIN>());
   uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(mt + (size_t)MT_COUNT * MT_N) +
                                                (sizeof(TIN) == 4 ? (size_t)MT_COUNT * MT_N * 4 : 0));
   unsigned char* stg = reinterpret_cast<unsigned char*>(bars + 8);
   __shared__ MxArgs sa;
   __shared__ int s_bx, s_by, s_bz, s_solve;
-  init_bars(bars);
+  init_bars<TJ>(bars);
   uint32_t tb = 0;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -530,7 +547,7 @@ __global__ void __launch_bounds__(TI * TJ, 2) mx_batch_kernel(const MxItem* __re
     }
     __syncthreads();
     const MxItem& B = solves[s_solve];
-    const int used = mx_item<KIND, MK, TIN>(&B.tin, &B.tp0, &B.tp1, sa, s_bx, s_by, s_bz, ring, mt, bars, tb, stg);
+    const int used = mx_item<KIND, MK, TIN, TJ>(&B.tin, &B.tp0, &B.tp1, sa, s_bx, s_by, s_bz, ring, mt, bars, tb, stg);
     if (used < 0) break;
     tb += (uint32_t)used;
     __syncthreads();
@@ -639,14 +656,13 @@ EncodeTiledFn enc_fn() {
 
 // 4-D view of a 5-variable state in element type of `esize` bytes (8 or 4):
 // x = elements along r (two per complex value), theta rows, phi planes, variables
-bool enc(CUtensorMap* tm, const Grid& g, const void* base, int esize, bool halo) {
+bool enc(CUtensorMap* tm, const Grid& g, const void* base, int esize, bool halo, int tj) {
   EncodeTiledFn fn = enc_fn();
   if (!fn) return false;
   const cuuint64_t cb = 2 * (cuuint64_t)esize;  // bytes per complex value
   cuuint64_t dims[4] = {(cuuint64_t)(2 * g.PI), (cuuint64_t)g.NJ, (cuuint64_t)g.NK, 5};
   cuuint64_t strides[3] = {(cuuint64_t)g.PI * cb, (cuuint64_t)g.plane * cb, (cuuint64_t)g.fs * cb};
-  cuuint32_t box[4] = {halo ? (cuuint32_t)RW : (cuuint32_t)(2 * TI), halo ? (cuuint32_t)RROWS : (cuuint32_t)TJ, 1,
-                       halo ? 5u : 5u};
+  cuuint32_t box[4] = {halo ? (cuuint32_t)RW : (cuuint32_t)(2 * TI), (cuuint32_t)(halo ? tj + 2 : tj), 1, 5u};
   cuuint32_t es[4] = {1, 1, 1, 1};
   return fn(tm, esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void*)base, dims,
             strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -659,14 +675,14 @@ int mx_chunk(const Grid& g) {
 }
 
 // maps and arguments of one solve's stage
-int mx_prepare(int kind, const MixedLaunch& L, const double* rsg, int* err, int kchunk, CUtensorMap* tin,
+int mx_prepare(int kind, const MixedLaunch& L, const double* rsg, int* err, int kchunk, int tj, CUtensorMap* tin,
                CUtensorMap* tp0, CUtensorMap* tp1, MxArgs* a) {
   const bool first = kind == ST_RK4_1;
-  if (!enc(tin, L.g, first ? (const void*)L.base : (const void*)L.in_f, first ? 8 : 4, true)) return -1;
+  if (!enc(tin, L.g, first ? (const void*)L.base : (const void*)L.in_f, first ? 8 : 4, true, tj)) return -1;
   int npf = 0;
   if (!first) {
-    if (enc(tp0, L.g, L.base, 8, false)) ++npf;
-    if (npf == 1 && enc(tp1, L.g, L.acc, 4, false)) ++npf;
+    if (enc(tp0, L.g, L.base, 8, false, tj)) ++npf;
+    if (npf == 1 && enc(tp1, L.g, L.acc, 4, false, tj)) ++npf;
   }
   if (npf < 2) *tp1 = *tin;
   if (npf < 1) *tp0 = *tin;
@@ -685,91 +701,102 @@ int mx_prepare(int kind, const MixedLaunch& L, const double* rsg, int* err, int 
   return 0;
 }
 
-template <int KIND, int MK, class TIN>
+template <int KIND, int MK, class TIN, int TJ>
 int mx_launch_one(const CUtensorMap& tin, const CUtensorMap& tp0, const CUtensorMap& tp1, const MxArgs& a,
                   cudaStream_t st) {
+  constexpr size_t SMEM = MGeom<TJ>::template smem<TIN>();
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(mx_stage_kernel<KIND, MK, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)mx_smem<TIN>()) != cudaSuccess)
+    if (cudaFuncSetAttribute(mx_stage_kernel<KIND, MK, TIN, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)SMEM) != cudaSuccess)
       return -1;
     attr = true;
   }
   const Grid& g = a.g;
   dim3 grid((g.NI + TI - 1) / TI, (g.NJ + TJ - 1) / TJ, (g.NK + a.kchunk - 1) / a.kchunk);
-  mx_stage_kernel<KIND, MK, TIN><<<grid, dim3(TI, TJ, 1), mx_smem<TIN>(), st>>>(tin, tp0, tp1, a);
+  mx_stage_kernel<KIND, MK, TIN, TJ><<<grid, dim3(TI, TJ, 1), SMEM, st>>>(tin, tp0, tp1, a);
   return 0;
 }
 
-template <int MK>
+template <int MK, int TJ>
 int mx_launch_mk(int kind, const CUtensorMap& tin, const CUtensorMap& tp0, const CUtensorMap& tp1, const MxArgs& a,
                  cudaStream_t st) {
   switch (kind) {
-    case ST_RK4_1: return mx_launch_one<ST_RK4_1, MK, double>(tin, tp0, tp1, a, st);
-    case ST_RK4_2: return mx_launch_one<ST_RK4_2, MK, float>(tin, tp0, tp1, a, st);
-    case ST_RK4_3: return mx_launch_one<ST_RK4_3, MK, float>(tin, tp0, tp1, a, st);
-    case ST_RK4_4: return mx_launch_one<ST_RK4_4, MK, float>(tin, tp0, tp1, a, st);
+    case ST_RK4_1: return mx_launch_one<ST_RK4_1, MK, double, TJ>(tin, tp0, tp1, a, st);
+    case ST_RK4_2: return mx_launch_one<ST_RK4_2, MK, float, TJ>(tin, tp0, tp1, a, st);
+    case ST_RK4_3: return mx_launch_one<ST_RK4_3, MK, float, TJ>(tin, tp0, tp1, a, st);
+    case ST_RK4_4: return mx_launch_one<ST_RK4_4, MK, float, TJ>(tin, tp0, tp1, a, st);
     default: return -1;
   }
 }
 
-template <int KIND, int MK, class TIN>
+template <int KIND, int MK, class TIN, int TJ>
 int mx_batch_one(const void* items, int n_solves, int n_items, int blocks, cudaStream_t st) {
+  constexpr size_t SMEM = MGeom<TJ>::template smem<TIN>();
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(mx_batch_kernel<KIND, MK, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)mx_smem<TIN>()) != cudaSuccess)
+    if (cudaFuncSetAttribute(mx_batch_kernel<KIND, MK, TIN, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)SMEM) != cudaSuccess)
       return -1;
     attr = true;
   }
   if (n_items <= 0) return 0;
-  mx_batch_kernel<KIND, MK, TIN><<<blocks, dim3(TI, TJ, 1), mx_smem<TIN>(), st>>>(
-      reinterpret_cast<const MxItem*>(items), n_solves, n_items);
+  mx_batch_kernel<KIND, MK, TIN, TJ><<<blocks, dim3(TI, TJ, 1), SMEM, st>>>(reinterpret_cast<const MxItem*>(items),
+                                                                           n_solves, n_items);
   return 0;
 }
 
-template <int MK>
+template <int MK, int TJ>
 int mx_batch_mk(int kind, const void* items, int n_solves, int n_items, int blocks, cudaStream_t st) {
   switch (kind) {
-    case ST_RK4_1: return mx_batch_one<ST_RK4_1, MK, double>(items, n_solves, n_items, blocks, st);
-    case ST_RK4_2: return mx_batch_one<ST_RK4_2, MK, float>(items, n_solves, n_items, blocks, st);
-    case ST_RK4_3: return mx_batch_one<ST_RK4_3, MK, float>(items, n_solves, n_items, blocks, st);
-    case ST_RK4_4: return mx_batch_one<ST_RK4_4, MK, float>(items, n_solves, n_items, blocks, st);
+    case ST_RK4_1: return mx_batch_one<ST_RK4_1, MK, double, TJ>(items, n_solves, n_items, blocks, st);
+    case ST_RK4_2: return mx_batch_one<ST_RK4_2, MK, float, TJ>(items, n_solves, n_items, blocks, st);
+    case ST_RK4_3: return mx_batch_one<ST_RK4_3, MK, float, TJ>(items, n_solves, n_items, blocks, st);
+    case ST_RK4_4: return mx_batch_one<ST_RK4_4, MK, float, TJ>(items, n_solves, n_items, blocks, st);
     default: return -1;
   }
 }
 
 }  // namespace
 
-int launch_stage_mixed(int kind, const MixedLaunch& L, const double* rsg, int* err, cudaStream_t st) {
+int launch_stage_mixed(int kind, const MixedLaunch& L, const double* rsg, int* err, cudaStream_t st, int tj) {
+  if (tj != 4) tj = 8;
   CUtensorMap tin, tp0, tp1;
   MxArgs a;
-  if (mx_prepare(kind, L, rsg, err, mx_chunk(L.g), &tin, &tp0, &tp1, &a)) return -1;
-  return L.metric_kind == MK_KS ? mx_launch_mk<MK_KS>(kind, tin, tp0, tp1, a, st)
-                                : mx_launch_mk<MK_SCHW>(kind, tin, tp0, tp1, a, st);
+  if (mx_prepare(kind, L, rsg, err, mx_chunk(L.g), tj, &tin, &tp0, &tp1, &a)) return -1;
+  if (tj == 4)
+    return L.metric_kind == MK_KS ? mx_launch_mk<MK_KS, 4>(kind, tin, tp0, tp1, a, st)
+                                  : mx_launch_mk<MK_SCHW, 4>(kind, tin, tp0, tp1, a, st);
+  return L.metric_kind == MK_KS ? mx_launch_mk<MK_KS, 8>(kind, tin, tp0, tp1, a, st)
+                                : mx_launch_mk<MK_SCHW, 8>(kind, tin, tp0, tp1, a, st);
 }
 
 size_t mixed_item_bytes() { return sizeof(MxItem); }
 
-int build_mixed_item(void* dst, int kind, const MixedLaunch& L, const double* rsg, int* err, int kchunk, int item0) {
+int build_mixed_item(void* dst, int kind, const MixedLaunch& L, const double* rsg, int* err, int kchunk, int item0,
+                     int tj) {
   {  // equal chunks of at most the requested length (as in the FP64 batch)
     const int nch = (L.g.NK + kchunk - 1) / kchunk;
     kchunk = (L.g.NK + nch - 1) / nch;
   }
   MxItem* B = reinterpret_cast<MxItem*>(dst);
   memset(B, 0, sizeof(MxItem));
-  if (mx_prepare(kind, L, rsg, err, kchunk, &B->tin, &B->tp0, &B->tp1, &B->a)) return -1;
+  if (mx_prepare(kind, L, rsg, err, kchunk, tj, &B->tin, &B->tp0, &B->tp1, &B->a)) return -1;
   B->tiles_x = (L.g.NI + TI - 1) / TI;
-  B->tiles_y = (L.g.NJ + TJ - 1) / TJ;
+  B->tiles_y = (L.g.NJ + tj - 1) / tj;
   B->item0 = item0;
   B->n_items = B->tiles_x * B->tiles_y * ((L.g.NK + kchunk - 1) / kchunk);
   return B->n_items;
 }
 
-int launch_batch_mixed(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks,
+int launch_batch_mixed(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks, int tj,
                        cudaStream_t st) {
-  return mk == MK_KS ? mx_batch_mk<MK_KS>(kind, d_items, n_solves, n_items, blocks, st)
-                     : mx_batch_mk<MK_SCHW>(kind, d_items, n_solves, n_items, blocks, st);
+  if (tj == 4)
+    return mk == MK_KS ? mx_batch_mk<MK_KS, 4>(kind, d_items, n_solves, n_items, blocks, st)
+                       : mx_batch_mk<MK_SCHW, 4>(kind, d_items, n_solves, n_items, blocks, st);
+  if (tj != 8) return -1;
+  return mk == MK_KS ? mx_batch_mk<MK_KS, 8>(kind, d_items, n_solves, n_items, blocks, st)
+                     : mx_batch_mk<MK_SCHW, 8>(kind, d_items, n_solves, n_items, blocks, st);
 }
 
 size_t ghost_f32_desc_bytes() { return sizeof(GhostF); }

@@ -35,21 +35,27 @@ namespace kg {
 using namespace tmaops;
 namespace {
 
-constexpr int TI = 32, TJ = 8, RH = 2;
+constexpr int TI = 32, RH = 2;
 template <bool B>
 struct TBool {
   static constexpr bool value = B;
 };
-constexpr int RW = 2 * (TI + 2 * RH);         // ring row width in doubles (72 = 576 B)
-constexpr int RROWS = TJ + 2;                 // theta rows with halo
-constexpr int FIELD_D = RROWS * RW;           // doubles per variable per plane
-constexpr int STAGE_D = 5 * FIELD_D;          // doubles per ring slot
-constexpr int STAGE_B = STAGE_D * 8;          // 28800 bytes
-constexpr int NST = 3;                        // ring depth
-constexpr int MW = TI + 2 * RH, MH = TJ + 2;  // metric tile
-constexpr int MT_N = MW * MH;
+constexpr int RW = 2 * (TI + 2 * RH);  // ring row width in doubles (72 = 576 B)
+constexpr int NST = 3;                 // ring depth
+constexpr int MW = TI + 2 * RH;        // metric tile width
 enum { MT_AL = 0, MT_BE, MT_A, MT_GRR, MT_GRP, MT_SG, MT_HT, MT_COUNT };
-constexpr size_t SMEM_BYTES = (size_t)NST * STAGE_B + (size_t)MT_COUNT * MT_N * 8 + 64 + 128;
+// tile geometry for TJ theta rows (one warp per row): 8 (256 threads, 2 CTAs
+// per SM) or 4 (128 threads, 3 CTAs per SM, twice the tiles of a grid)
+template <int TJ>
+struct Geom {
+  static constexpr int RROWS = TJ + 2;             // theta rows with halo
+  static constexpr int FIELD_D = RROWS * RW;       // doubles per variable per plane
+  static constexpr int STAGE_D = 5 * FIELD_D;      // doubles per ring slot
+  static constexpr int STAGE_B = STAGE_D * 8;      // 28800 bytes at TJ = 8
+  static constexpr int MH = TJ + 2, MT_N = MW * MH;  // metric tile
+  static constexpr size_t SMEM_BYTES = (size_t)NST * STAGE_B + (size_t)MT_COUNT * MT_N * 8 + 64 + 128;
+  static constexpr int MIN_BLOCKS = TJ == 4 ? 3 : 2;
+};
 __device__ __forceinline__ double ddiv(double a, double b, double rb) {
   const double q = a * rb;
   const double r = __fma_rn(-q, b, a);
@@ -89,10 +95,12 @@ struct alignas(64) BatchItem {
 // `tb` counts the planes this CTA has already pulled through its ring (ring
 // slot and mbarrier parity continue across items in the persistent kernel).
 // Returns the number of planes consumed, or -1 when a bounded wait ran out.
-template <int KIND, int MK>
+template <int KIND, int MK, int TJ>
 __device__ __forceinline__ int stage_item(const CUtensorMap* tm4p, const CUtensorMap* tm1p, const CUtensorMap* tp0p,
                                           const CUtensorMap* tp1p, const TmaArgs& a, int bx, int by, int bz,
                                           double* ring, double* mt, uint64_t* bars, uint32_t tb) {
+  using GT = Geom<TJ>;
+  constexpr int FIELD_D = GT::FIELD_D, STAGE_D = GT::STAGE_D, STAGE_B = GT::STAGE_B, MT_N = GT::MT_N;
   constexpr bool PSI = (KIND != ST_P2_S1B && KIND != ST_P3_S2B);
   constexpr bool PI_ = (KIND != ST_P2_S1A && KIND != ST_P3_S2A);
   const Grid& g = a.g;
@@ -420,42 +428,43 @@ __device__ __forceinline__ unsigned char* align128(unsigned char* p) {
   return p + ((128u - (a & 127u)) & 127u);
 }
 
+template <int TJ>
 __device__ __forceinline__ void init_ring_barriers(uint64_t* bars) {
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
-    for (int s = 0; s < NST; ++s) mbar_init(&bars[NST + s], TI * TJ / 32);
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[NST + s], TJ);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 }
 
-template <int KIND, int MK>
-__global__ void __launch_bounds__(TI * TJ, 2)
+template <int KIND, int MK, int TJ>
+__global__ void __launch_bounds__(TI * TJ, Geom<TJ>::MIN_BLOCKS)
     tma_stage_kernel(const __grid_constant__ CUtensorMap tm4, const __grid_constant__ CUtensorMap tm1,
                      const __grid_constant__ CUtensorMap tp0, const __grid_constant__ CUtensorMap tp1, TmaArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* ring = reinterpret_cast<double*>(align128(smem_raw));
-  double* mt = ring + (size_t)NST * STAGE_D;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
+  double* mt = ring + (size_t)NST * Geom<TJ>::STAGE_D;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * Geom<TJ>::MT_N);
   if ((int)blockIdx.z * a.kchunk >= a.g.NK) return;
-  init_ring_barriers(bars);
-  (void)stage_item<KIND, MK>(&tm4, &tm1, &tp0, &tp1, a, blockIdx.x, blockIdx.y, blockIdx.z, ring, mt, bars, 0u);
+  init_ring_barriers<TJ>(bars);
+  (void)stage_item<KIND, MK, TJ>(&tm4, &tm1, &tp0, &tp1, a, blockIdx.x, blockIdx.y, blockIdx.z, ring, mt, bars, 0u);
 }
 
 // ---- persistent kernel over many solves -------------------------------------
 // Every solve of a batch contributes tiles_x * tiles_y * chunks work items; a
 // CTA walks the ragged list item = blockIdx.x, blockIdx.x + gridDim.x, ...
 // and runs each with the solve's own grid, metric, buffers and tensor maps.
-template <int KIND, int MK>
-__global__ void __launch_bounds__(TI * TJ, 2) tma_batch_kernel(const BatchItem* __restrict__ solves, int n_solves,
-                                                                 int n_items) {
+template <int KIND, int MK, int TJ>
+__global__ void __launch_bounds__(TI * TJ, Geom<TJ>::MIN_BLOCKS)
+    tma_batch_kernel(const BatchItem* __restrict__ solves, int n_solves, int n_items) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* ring = reinterpret_cast<double*>(align128(smem_raw));
-  double* mt = ring + (size_t)NST * STAGE_D;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * MT_N);
+  double* mt = ring + (size_t)NST * Geom<TJ>::STAGE_D;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mt + (size_t)MT_COUNT * Geom<TJ>::MT_N);
   __shared__ TmaArgs sa;
   __shared__ int s_bx, s_by, s_bz, s_solve;
-  init_ring_barriers(bars);
+  init_ring_barriers<TJ>(bars);
   uint32_t tb = 0;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -475,7 +484,7 @@ __global__ void __launch_bounds__(TI * TJ, 2) tma_batch_kernel(const BatchItem* 
     }
     __syncthreads();
     const BatchItem& B = solves[s_solve];
-    const int used = stage_item<KIND, MK>(&B.tm4, &B.tm1, &B.tp0, &B.tp1, sa, s_bx, s_by, s_bz, ring, mt, bars, tb);
+    const int used = stage_item<KIND, MK, TJ>(&B.tm4, &B.tm1, &B.tp0, &B.tp1, sa, s_bx, s_by, s_bz, ring, mt, bars, tb);
     if (used < 0) break;
     tb += (uint32_t)used;
     __syncthreads();  // sa and the item indices are rewritten for the next item
@@ -502,13 +511,14 @@ EncodeTiledFn encode_fn() {
 }
 
 // 4-D view (x = doubles along r incl. row padding, theta rows, phi planes, variables);
-// halo = true: the stencil box (tile + r halo 2 + theta halo 1), false: the tile
-bool encode(CUtensorMap* tm, const Grid& g, const double2* base, int nvars, bool halo = true) {
+// halo = true: the stencil box (tile + r halo 2 + theta halo 1), false: the tile;
+// tj: theta rows of the tile
+bool encode(CUtensorMap* tm, const Grid& g, const double2* base, int nvars, bool halo = true, int tj = 8) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[4] = {(cuuint64_t)(2 * g.PI), (cuuint64_t)g.NJ, (cuuint64_t)g.NK, (cuuint64_t)nvars};
   cuuint64_t strides[3] = {(cuuint64_t)g.PI * 16, (cuuint64_t)g.plane * 16, (cuuint64_t)g.fs * 16};
-  cuuint32_t box[4] = {halo ? (cuuint32_t)RW : (cuuint32_t)(2 * TI), halo ? (cuuint32_t)RROWS : (cuuint32_t)TJ, 1,
+  cuuint32_t box[4] = {halo ? (cuuint32_t)RW : (cuuint32_t)(2 * TI), (cuuint32_t)(halo ? tj + 2 : tj), 1,
                        (cuuint32_t)nvars};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)base, dims, strides, box, estr,
@@ -526,25 +536,34 @@ struct Maps {
   CUtensorMap tm4, tm1, tp0, tp1;
 };
 
-template <int KIND, int MK>
+template <int KIND, int MK, int TJ>
 int launch_one(const Maps& m, const TmaArgs& a, cudaStream_t st) {
+  constexpr size_t SMEM = Geom<TJ>::SMEM_BYTES;
   static bool attr_set = false;
   if (!attr_set) {
-    if (cudaFuncSetAttribute(tma_stage_kernel<KIND, MK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)SMEM_BYTES) != cudaSuccess)
+    if (cudaFuncSetAttribute(tma_stage_kernel<KIND, MK, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)SMEM) != cudaSuccess)
       return -1;
     attr_set = true;
   }
   const Grid& g = a.g;
   dim3 block(TI, TJ, 1);
   dim3 grid((g.NI + TI - 1) / TI, (g.NJ + TJ - 1) / TJ, (g.NK + a.kchunk - 1) / a.kchunk);
-  tma_stage_kernel<KIND, MK><<<grid, block, SMEM_BYTES, st>>>(m.tm4, m.tm1, m.tp0, m.tp1, a);
+  tma_stage_kernel<KIND, MK, TJ><<<grid, block, SMEM, st>>>(m.tm4, m.tm1, m.tp0, m.tp1, a);
   return 0;
 }
 
+// the 4-row tiles are built for the RK4 stages (the batched forms' stepper) only
 template <int KIND>
-int launch_kind(const Maps& m, const TmaArgs& a, int mk, cudaStream_t st) {
-  return mk == MK_KS ? launch_one<KIND, MK_KS>(m, a, st) : launch_one<KIND, MK_SCHW>(m, a, st);
+constexpr bool has_tj4() {
+  return KIND == ST_RK4_1 || KIND == ST_RK4_2 || KIND == ST_RK4_3 || KIND == ST_RK4_4;
+}
+template <int KIND>
+int launch_kind(const Maps& m, const TmaArgs& a, int mk, int tj, cudaStream_t st) {
+  if constexpr (has_tj4<KIND>()) {
+    if (tj == 4) return mk == MK_KS ? launch_one<KIND, MK_KS, 4>(m, a, st) : launch_one<KIND, MK_SCHW, 4>(m, a, st);
+  }
+  return mk == MK_KS ? launch_one<KIND, MK_KS, 8>(m, a, st) : launch_one<KIND, MK_SCHW, 8>(m, a, st);
 }
 
 }  // namespace
@@ -552,8 +571,8 @@ int launch_kind(const Maps& m, const TmaArgs& a, int mk, cudaStream_t st) {
 size_t batch_item_bytes() { return sizeof(BatchItem); }
 
 // fill one solve's item record for a batched launch of stage `kind`
-int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rsg, int* err, int kchunk,
-                     int item0) {
+int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rsg, int* err, int kchunk, int item0,
+                     int tj) {
   // the requested chunk length is an upper bound: the solve's planes are split
   // into equal chunks, so no chunk is a short remainder that pays a whole
   // pipeline prologue for a few planes
@@ -563,7 +582,7 @@ int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rs
   }
   BatchItem* B = reinterpret_cast<BatchItem*>(dst);
   memset(B, 0, sizeof(BatchItem));
-  if (!encode(&B->tm4, L.g, L.in[0], 4) || !encode(&B->tm1, L.g, L.in[4], 1)) return -1;
+  if (!encode(&B->tm4, L.g, L.in[0], 4, true, tj) || !encode(&B->tm1, L.g, L.in[4], 1, true, tj)) return -1;
   const long long fsl = L.g.fs;
   int base_in = 1;
   for (int v = 0; v < 5; ++v) base_in = base_in && (L.in[v] == L.base + v * fsl);
@@ -571,7 +590,7 @@ int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rs
   int npf = 0;
   auto add = [&](const double2* p, int nv) {
     CUtensorMap* t = npf == 0 ? &B->tp0 : &B->tp1;
-    if (npf < 2 && p && encode(t, L.g, p, nv, false)) ++npf;
+    if (npf < 2 && p && encode(t, L.g, p, nv, false, tj)) ++npf;
   };
   if (!base_in) {
     switch (kind) {
@@ -600,7 +619,7 @@ int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rs
   a.npf = npf;
   a.base_in = base_in;
   B->tiles_x = (L.g.NI + TI - 1) / TI;
-  B->tiles_y = (L.g.NJ + TJ - 1) / TJ;
+  B->tiles_y = (L.g.NJ + tj - 1) / tj;
   const int chunks = (L.g.NK + kchunk - 1) / kchunk;
   B->item0 = item0;
   B->n_items = B->tiles_x * B->tiles_y * chunks;
@@ -608,36 +627,44 @@ int build_batch_item(void* dst, int kind, const StageLaunch& L, const double* rs
 }
 
 namespace {
-template <int KIND, int MK>
+template <int KIND, int MK, int TJ>
 int batch_one(const void* items, int n_solves, int n_items, int blocks, cudaStream_t st) {
+  constexpr size_t SMEM = Geom<TJ>::SMEM_BYTES;
   static bool attr_set = false;
   if (!attr_set) {
-    if (cudaFuncSetAttribute(tma_batch_kernel<KIND, MK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)SMEM_BYTES) != cudaSuccess)
+    if (cudaFuncSetAttribute(tma_batch_kernel<KIND, MK, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)SMEM) != cudaSuccess)
       return -1;
     attr_set = true;
   }
   if (n_items <= 0) return 0;
-  tma_batch_kernel<KIND, MK><<<blocks, dim3(TI, TJ, 1), SMEM_BYTES, st>>>(
-      reinterpret_cast<const BatchItem*>(items), n_solves, n_items);
+  tma_batch_kernel<KIND, MK, TJ><<<blocks, dim3(TI, TJ, 1), SMEM, st>>>(reinterpret_cast<const BatchItem*>(items),
+                                                                       n_solves, n_items);
   return 0;
 }
 template <int KIND>
-int batch_kind(const void* items, int n_solves, int n_items, int blocks, int mk, cudaStream_t st) {
-  return mk == MK_KS ? batch_one<KIND, MK_KS>(items, n_solves, n_items, blocks, st)
-                     : batch_one<KIND, MK_SCHW>(items, n_solves, n_items, blocks, st);
+int batch_kind(const void* items, int n_solves, int n_items, int blocks, int mk, int tj, cudaStream_t st) {
+  if constexpr (has_tj4<KIND>()) {
+    if (tj == 4)
+      return mk == MK_KS ? batch_one<KIND, MK_KS, 4>(items, n_solves, n_items, blocks, st)
+                         : batch_one<KIND, MK_SCHW, 4>(items, n_solves, n_items, blocks, st);
+  }
+  if (tj != 8) return -1;
+  return mk == MK_KS ? batch_one<KIND, MK_KS, 8>(items, n_solves, n_items, blocks, st)
+                     : batch_one<KIND, MK_SCHW, 8>(items, n_solves, n_items, blocks, st);
 }
 }  // namespace
 
-int launch_batch_tma(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks, cudaStream_t st) {
+int launch_batch_tma(int kind, int mk, const void* d_items, int n_solves, int n_items, int blocks, int tj,
+                     cudaStream_t st) {
   switch (kind) {
-    case ST_P2_S1A: return batch_kind<ST_P2_S1A>(d_items, n_solves, n_items, blocks, mk, st);
-    case ST_P2_S1B: return batch_kind<ST_P2_S1B>(d_items, n_solves, n_items, blocks, mk, st);
-    case ST_P2_S2: return batch_kind<ST_P2_S2>(d_items, n_solves, n_items, blocks, mk, st);
-    case ST_RK4_1: return batch_kind<ST_RK4_1>(d_items, n_solves, n_items, blocks, mk, st);
-    case ST_RK4_2: return batch_kind<ST_RK4_2>(d_items, n_solves, n_items, blocks, mk, st);
-    case ST_RK4_3: return batch_kind<ST_RK4_3>(d_items, n_solves, n_items, blocks, mk, st);
-    case ST_RK4_4: return batch_kind<ST_RK4_4>(d_items, n_solves, n_items, blocks, mk, st);
+    case ST_P2_S1A: return batch_kind<ST_P2_S1A>(d_items, n_solves, n_items, blocks, mk, tj, st);
+    case ST_P2_S1B: return batch_kind<ST_P2_S1B>(d_items, n_solves, n_items, blocks, mk, tj, st);
+    case ST_P2_S2: return batch_kind<ST_P2_S2>(d_items, n_solves, n_items, blocks, mk, tj, st);
+    case ST_RK4_1: return batch_kind<ST_RK4_1>(d_items, n_solves, n_items, blocks, mk, tj, st);
+    case ST_RK4_2: return batch_kind<ST_RK4_2>(d_items, n_solves, n_items, blocks, mk, tj, st);
+    case ST_RK4_3: return batch_kind<ST_RK4_3>(d_items, n_solves, n_items, blocks, mk, tj, st);
+    case ST_RK4_4: return batch_kind<ST_RK4_4>(d_items, n_solves, n_items, blocks, mk, tj, st);
     default: return -1;
   }
 }
@@ -647,15 +674,17 @@ bool tma_available(const Grid& g, const double2* some_state) {
   return encode(&tm, g, some_state, 4) && encode(&tm, g, some_state, 1);
 }
 
-int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st) {
+int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err, cudaStream_t st, int tj) {
+  const bool rk4 = kind == ST_RK4_1 || kind == ST_RK4_2 || kind == ST_RK4_3 || kind == ST_RK4_4;
+  if (!rk4 || tj != 4) tj = 8;  // the 4-row tiles exist for the RK4 stages
   Maps mp;
-  if (!encode(&mp.tm4, L.g, L.in[0], 4) || !encode(&mp.tm1, L.g, L.in[4], 1)) return -1;
+  if (!encode(&mp.tm4, L.g, L.in[0], 4, true, tj) || !encode(&mp.tm1, L.g, L.in[4], 1, true, tj)) return -1;
   // point-wise operands read in the combination, prefetched into L2
   int npf = 0;
   const long long fs = L.g.fs;
   auto add = [&](const double2* p, int nv) {
     CUtensorMap* t = npf == 0 ? &mp.tp0 : &mp.tp1;
-    if (npf < 2 && p && encode(t, L.g, p, nv, false)) ++npf;
+    if (npf < 2 && p && encode(t, L.g, p, nv, false, tj)) ++npf;
   };
   const long long fsl = L.g.fs;
   int base_in = 1;
@@ -688,19 +717,19 @@ int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err
   if (npf < 1) mp.tp0 = mp.tm1;
   const int mk = L.metric_kind;
   switch (kind) {
-    case ST_P2_S1A: return launch_kind<ST_P2_S1A>(mp, a, mk, st);
-    case ST_P2_S1B: return launch_kind<ST_P2_S1B>(mp, a, mk, st);
-    case ST_P2_S2: return launch_kind<ST_P2_S2>(mp, a, mk, st);
-    case ST_P3_S2A: return launch_kind<ST_P3_S2A>(mp, a, mk, st);
-    case ST_P3_S2B: return launch_kind<ST_P3_S2B>(mp, a, mk, st);
-    case ST_P3_S3: return launch_kind<ST_P3_S3>(mp, a, mk, st);
-    case ST_RK3_1: return launch_kind<ST_RK3_1>(mp, a, mk, st);
-    case ST_RK3_2: return launch_kind<ST_RK3_2>(mp, a, mk, st);
-    case ST_RK3_3: return launch_kind<ST_RK3_3>(mp, a, mk, st);
-    case ST_RK4_1: return launch_kind<ST_RK4_1>(mp, a, mk, st);
-    case ST_RK4_2: return launch_kind<ST_RK4_2>(mp, a, mk, st);
-    case ST_RK4_3: return launch_kind<ST_RK4_3>(mp, a, mk, st);
-    case ST_RK4_4: return launch_kind<ST_RK4_4>(mp, a, mk, st);
+    case ST_P2_S1A: return launch_kind<ST_P2_S1A>(mp, a, mk, tj, st);
+    case ST_P2_S1B: return launch_kind<ST_P2_S1B>(mp, a, mk, tj, st);
+    case ST_P2_S2: return launch_kind<ST_P2_S2>(mp, a, mk, tj, st);
+    case ST_P3_S2A: return launch_kind<ST_P3_S2A>(mp, a, mk, tj, st);
+    case ST_P3_S2B: return launch_kind<ST_P3_S2B>(mp, a, mk, tj, st);
+    case ST_P3_S3: return launch_kind<ST_P3_S3>(mp, a, mk, tj, st);
+    case ST_RK3_1: return launch_kind<ST_RK3_1>(mp, a, mk, tj, st);
+    case ST_RK3_2: return launch_kind<ST_RK3_2>(mp, a, mk, tj, st);
+    case ST_RK3_3: return launch_kind<ST_RK3_3>(mp, a, mk, tj, st);
+    case ST_RK4_1: return launch_kind<ST_RK4_1>(mp, a, mk, tj, st);
+    case ST_RK4_2: return launch_kind<ST_RK4_2>(mp, a, mk, tj, st);
+    case ST_RK4_3: return launch_kind<ST_RK4_3>(mp, a, mk, tj, st);
+    case ST_RK4_4: return launch_kind<ST_RK4_4>(mp, a, mk, tj, st);
     default: return -1;
   }
 }

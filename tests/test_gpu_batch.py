@@ -132,3 +132,28 @@ def test_concurrent_dispatch_mixed_matches_persistent():
         out.append([m.u for m in ms])
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("dispatch", [0, 1])
+def test_tile_rows_4_matches_solo(precision, dispatch):
+    """32 x 4 tiles in the persistent launch and in the concurrent members'
+    kernels: the bits of each solve stepped alone in 32 x 8 tiles"""
+    from kg_b200.batch import Batch
+    batch = Batch(precision=precision)
+    batch.set_tuning(16, 444, dispatch, 2 if dispatch else -1, 4)
+    assert batch.tuning().tile_rows == 4
+    members, solos = [], []
+    for sp in SHAPES:
+        m, _ = _solve(sp)
+        s, _ = _solve(sp)
+        s.precision = precision
+        batch.add(m)
+        members.append(m)
+        solos.append(s)
+    batch.rk4(5)
+    batch.synchronize()
+    for s in solos:
+        s.rk4(nsteps=5)
+    for m, s in zip(members, solos):
+        assert np.array_equal(m.u, s.u)

@@ -86,3 +86,14 @@ def test_mixed_waveform_error_at_detectors():
     err = _rel(wb, wa)
     print(f"waveform rel L2 error (300 steps, l<=8, 3 detectors): {err:.2e}")
     assert err <= 1e-6
+
+
+def test_mixed_tile_rows_same_bits():
+    """the mixed stages in 32 x 4 tiles give the bits of the 32 x 8 tiles"""
+    out = []
+    for rows in (8, 4):
+        s = _solve(SHAPES[1], "mixed")
+        s._ck(s._lib.kg_set_tile_rows(s.handle, rows))
+        s.rk4(nsteps=6)
+        out.append(s.u)
+    assert np.array_equal(out[0], out[1])

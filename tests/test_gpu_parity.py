@@ -298,3 +298,22 @@ def test_profile_and_launch_count():
     dev._ck(dev._lib.kg_profile_read(dev.handle, ms, cnt))
     assert dev._lib.kg_launch_count(dev.handle) - n0 == 2 * 5
     assert cnt[0] == 2 and cnt[1] == 2 and cnt[names.index("stage_pirk_s1_fused")] == 0
+
+
+@pytest.mark.parametrize("grid", [SMALL, dict(Nx=61, Ny=13, Nz=41, xmin=1.8, xmax=30.0),
+                                  dict(Nx=12, Ny=7, Nz=8, xmin=1.8, xmax=9.0)])
+@pytest.mark.parametrize("metric,bc", [("Kerr_Schild", "outflow"), ("Schw_EF", "inflow")])
+def test_rk4_tile_rows_4_bitexact(grid, metric, bc):
+    """RK4 stage kernels in 32 x 4 tiles (kg_set_tile_rows): the oracle's bits,
+    on grids whose theta extent leaves a partial last tile of 4 rows"""
+    dev, ora = _pair(grid=grid, metric=metric, bc=bc)
+    dev._ck(dev._lib.kg_set_tile_rows(dev.handle, 4))
+    assert dev._lib.kg_get_tile_rows(dev.handle) == 4
+    assert dev._lib.kg_set_tile_rows(dev.handle, 6) != 0
+    from kg_b200.initial_data import shell_ylm
+    u0, _ = shell_ylm(grid["Nx"], grid["Ny"], grid["Nz"], grid["xmin"], grid["xmax"], seed=4, r0=5.0, sd=1.0)
+    dev.u = u0
+    ora.set_state(u0)
+    dev.rk4(nsteps=3)
+    ora.rk4(3)
+    assert np.array_equal(dev.u, ora.get_state())

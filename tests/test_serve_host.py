@@ -126,13 +126,20 @@ def test_request_larger_than_budget_is_refused(served):
 
 def test_tuner_candidates_cover_both_dispatches():
     """the batch tuner's search space (host logic): persistent launches over
-    (kchunk, CTAs per SM) and concurrent single-solve launches over the
-    stage-kernel forms; the mixed form has the TMA form only"""
+    (kchunk, CTAs per SM, tile rows) and concurrent single-solve launches over the
+    stage-kernel forms, the TMA form in both tile heights; the mixed form has the
+    TMA form only"""
     from kg_b200.batch import Tuning, candidates
     c64 = candidates("fp64", kchunks=(16, 32), ctas_per_sm=(1, 2), sms=148)
     assert Tuning(16, 148, 0, -1) in c64 and Tuning(32, 296, 0, -1) in c64
+    # 32 x 4 tiles: 1.5x the CTAs per SM of the 32 x 8 candidates
+    assert Tuning(16, 148, 0, -1, 4) in c64 and Tuning(32, 444, 0, -1, 4) in c64
     assert {t.variant for t in c64 if t.dispatch == 1} == {0, 1, 2}
+    assert {t.tile_rows for t in c64 if t.dispatch == 1 and t.variant == 2} == {8, 4}
+    assert {t.tile_rows for t in c64 if t.dispatch == 1 and t.variant != 2} == {8}
     cmx = candidates("mixed", kchunks=(16,), ctas_per_sm=(2,), sms=148)
-    assert {t.variant for t in cmx if t.dispatch == 1} == {2}
+    assert {(t.variant, t.tile_rows) for t in cmx if t.dispatch == 1} == {(2, 8), (2, 4)}
+    assert len(candidates("fp64", kchunks=(16,), ctas_per_sm=(2,), tile_rows=(8,))) == 1 + 3
     t = Tuning(8, 37, 1, 2)
-    assert (t.kchunk, t.blocks, t.dispatch, t.variant) == (8, 37, 1, 2) and tuple(t) == (8, 37, 1, 2)
+    assert (t.kchunk, t.blocks, t.dispatch, t.variant, t.tile_rows) == (8, 37, 1, 2, 8)
+    assert tuple(t) == (8, 37, 1, 2, 8)
