@@ -136,7 +136,10 @@ namespace {
 
 // RHS of all five variables at the thread's own point, arithmetic in R.
 // cu: ring slot of plane k; E/F: phi-derivative arguments at k-1 and k+1.
-template <class R, int MK, class TIN, int TJ>
+// FAST: every lane of the warp lies two points inside the array in r with
+// beta^r > 0 (in R), so every lane takes the centred derivative and the forward
+// upwind difference -- the branches the general form takes there
+template <class R, int MK, class TIN, int TJ, bool FAST = false>
 __device__ __forceinline__ void mx_rhs(const MxArgs& a, const TIN* cu, const double* mt, const float* mtf, int tx,
                                        int ty, int ii, int jj, int k, const double* own, double2 Epv, double2 Enx,
                                        double2 Fpv, double2 Fnx, cx<R> r[5]) {
@@ -167,12 +170,14 @@ __device__ __forceinline__ void mx_rhs(const MxArgs& a, const TIN* cu, const dou
     auto aPi = [&](int dx) { return sm(MTV(MT_AL, tx + dx, ty), RF(4, tx + dx, ty)); };
     auto ps1 = [&](int dx) { return RF(1, tx + dx, ty); };
     cx<R> d;
-    if (ii == 0) d = f3(aPi(0), aPi(1), aPi(2));
+    if (FAST) d = cc(aPi(-1), aPi(1));
+    else if (ii == 0) d = f3(aPi(0), aPi(1), aPi(2));
     else if (ii == n) d = b3(aPi(0), aPi(-1), aPi(-2));
     else d = cc(aPi(-1), aPi(1));
     d = sm(rdx, d);
     cx<R> av;
-    if (ii <= 1) av = f3(fcu[1], ps1(1), ps1(2));
+    if (FAST) av = f3(fcu[1], ps1(1), ps1(2));
+    else if (ii <= 1) av = f3(fcu[1], ps1(1), ps1(2));
     else if (ii == n - 1) av = sub(ps1(1), ps1(-1));
     else if (ii == n) av = b3(fcu[1], ps1(-1), ps1(-2));
     else if (be > (R)0) av = f3(fcu[1], ps1(1), ps1(2));
@@ -215,7 +220,8 @@ __device__ __forceinline__ void mx_rhs(const MxArgs& a, const TIN* cu, const dou
       return sm(MTV(MT_A, tx + dx, ty), RF(1, tx + dx, ty));
     };
     cx<R> d;
-    if (ii == 0) d = f3(G1(0), G1(1), G1(2));
+    if (FAST) d = cc(G1(-1), G1(1));
+    else if (ii == 0) d = f3(G1(0), G1(1), G1(2));
     else if (ii == n) d = b3(G1(0), G1(-1), G1(-2));
     else d = cc(G1(-1), G1(1));
     const cx<R> r1 = dsg(sm(rdx, d), sg, rs);
@@ -236,7 +242,8 @@ __device__ __forceinline__ void mx_rhs(const MxArgs& a, const TIN* cu, const dou
     const cx<R> r4 = sm(dxb, fcu[4]);
     auto Q = [&](int dx) { return sm(MTV(MT_SG, tx + dx, ty), RF(4, tx + dx, ty)); };
     cx<R> av;
-    if (ii <= 1) av = f3(Q(0), Q(1), Q(2));
+    if (FAST) av = f3(Q(0), Q(1), Q(2));
+    else if (ii <= 1) av = f3(Q(0), Q(1), Q(2));
     else if (ii == n - 1) av = sub(Q(1), Q(-1));
     else if (ii == n) av = b3(Q(0), Q(-1), Q(-2));
     else if (be > (R)0) av = f3(Q(0), Q(1), Q(2));
@@ -360,6 +367,8 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
   }
   // FP64 RHS at the excision side and next to the poles
   const bool hp = (ii <= 1) || (jj <= 1) || (jj >= g.NJ - 2);
+  const bool fast =
+      __all_sync(0xffffffffu, act && !hp && ii <= g.NI - 3 && (float)own[1] > 0.0f);  // warp-uniform
   auto EF = [&](const TIN* st, double2& E, double2& F) {
     if (hp) mx_EF<double, MK, TIN, TJ>(st, tx, ty, own, E, F);
     else mx_EF<float, MK, TIN, TJ>(st, tx, ty, own, E, F);
@@ -416,7 +425,8 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
         for (int v = 0; v < 5; ++v) rr[v] = make_double2(r[v].x, r[v].y);
       } else {
         cx<float> r[5];
-        mx_rhs<float, MK, TIN, TJ>(a, cu, mt, mtf, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
+        if (fast) mx_rhs<float, MK, TIN, TJ, true>(a, cu, mt, mtf, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
+        else mx_rhs<float, MK, TIN, TJ, false>(a, cu, mt, mtf, tx, ty, ii, jj, k, own, Epv, Enx, Fpv, Fnx, r);
 #pragma unroll
         for (int v = 0; v < 5; ++v) rr[v] = make_double2((double)r[v].x, (double)r[v].y);
       }
