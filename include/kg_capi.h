@@ -235,6 +235,14 @@ int kg_set_kernel_variant(kg_solver *h, int variant);
  * SM, twice the tiles per grid).  The same bits either way.  No reference
  * counterpart. */
 int kg_set_tile_rows(kg_solver *h, int rows);
+/* No reference counterpart (the reference stops on errors).  Exercises the
+ * failure path every TMA-fed kernel takes when a bounded wait runs out, without
+ * a fault: one warp waits, at most `polls` (1..2^20) polls, on an mbarrier phase
+ * that nothing completes, sets the handle's device error flag and returns.  The
+ * call returns KG_ETIMEOUT with the message of a stage launch whose copies never
+ * landed, then clears the flag, so the handle and its context stay usable.  (A
+ * flag already set by an earlier launch is reported and left set.) */
+int kg_check_wait_timeout(kg_solver *h, long long polls);
 int kg_get_tile_rows(const kg_solver *h);
 
 /* --- batched engine ------------------------------------------------------------ */

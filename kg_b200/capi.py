@@ -90,6 +90,7 @@ SIGNATURES = [
     ("kg_launch_count", C.c_longlong, [_P]),
     ("kg_set_kernel_variant", _I, [_P, _I]),
     ("kg_set_tile_rows", _I, [_P, _I]),
+    ("kg_check_wait_timeout", _I, [_P, C.c_longlong]),
     ("kg_get_tile_rows", _I, [_P]),
     ("kg_batch_create", _I, [_I, _PP]),
     ("kg_batch_destroy", _I, [_P]),

@@ -1936,6 +1936,20 @@ int kg_set_kernel_variant(kg_solver* h, int variant) {
   return KG_OK;
 }
 
+int kg_check_wait_timeout(kg_solver* h, long long polls) {
+  if (!h || polls < 1 || polls > (1LL << 20)) return KG_EINVAL;
+  KG_CK(cudaStreamSynchronize(h->stream));
+  int rc = check_device_flag(h);
+  if (rc) return rc;  // an earlier wait ran out: report that one
+  if (kg::launch_wait_check(h->derr, polls, h->stream)) return set_err(h, KG_ECUDA, "wait check launch failed");
+  rc = check_device_flag(h);  // KG_ETIMEOUT, with the message of a stage launch whose copies never landed
+  if (rc != KG_ETIMEOUT) return rc ? rc : set_err(h, KG_ECUDA, "the bounded wait did not run out");
+  // clear the flag: the CTA left nothing in flight, so the handle stays usable
+  KG_CK(cudaMemsetAsync(h->derr, 0, sizeof(int), h->stream));
+  KG_CK(cudaStreamSynchronize(h->stream));
+  return KG_ETIMEOUT;
+}
+
 int kg_set_tile_rows(kg_solver* h, int rows) {
   if (!h || (rows != 4 && rows != 8)) return KG_EINVAL;
   if (rows != h->tile_rows) {

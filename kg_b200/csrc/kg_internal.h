@@ -47,6 +47,9 @@ int launch_stage_tma(int kind, const StageLaunch& L, const double* rsg, int* err
 // dt rhs_pi(S(1:4), Sold).  Returns -1 if the tensor maps cannot be encoded.
 int launch_pirk_s1_fused(const Grid& g, const Metric& m, int mk, const double2* U, const double2* Sold, double2* S,
                          double2* Snew, const double* rsg, int* err, cudaStream_t st);
+// one warp waits at most `polls` polls on an mbarrier phase that never completes,
+// then sets *err (the failure path of every bounded wait); returns -1 if the launch fails
+int launch_wait_check(int* err, long long polls, cudaStream_t st);
 // true when the driver can encode the tensor maps the TMA form needs for this grid
 bool tma_available(const Grid& g, const double2* some_state);
 // batched (multi-solve) persistent launches of the TMA stage kernel

@@ -669,6 +669,26 @@ int launch_batch_tma(int kind, int mk, const void* d_items, int n_solves, int n_
   }
 }
 
+// The failure path of a bounded wait, on its own: one warp waits, at most
+// `polls` polls, on the first phase of an mbarrier that nothing arrives on and
+// no copy completes, then sets the error flag and returns -- what a stage
+// kernel does when its copies never land.  Nothing is left in flight.
+__global__ void wait_check_kernel(int* err, long long polls) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  const bool ok = mbar_wait_bounded_n(&bar, 0u, polls);
+  if (__any_sync(0xffffffffu, !ok) && threadIdx.x == 0) atomicExch(err, 1);
+}
+
+int launch_wait_check(int* err, long long polls, cudaStream_t st) {
+  wait_check_kernel<<<1, 32, 0, st>>>(err, polls);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 bool tma_available(const Grid& g, const double2* some_state) {
   CUtensorMap tm;
   return encode(&tm, g, some_state, 4) && encode(&tm, g, some_state, 1);

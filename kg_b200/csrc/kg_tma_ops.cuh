@@ -33,10 +33,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity) {
-  for (long long it = 0; it < WAIT_LIMIT; ++it)
+__device__ __forceinline__ bool mbar_wait_bounded_n(uint64_t* b, uint32_t parity, long long limit) {
+  for (long long it = 0; it < limit; ++it)
     if (mbar_try_wait(b, parity)) return true;
   return false;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity) {
+  return mbar_wait_bounded_n(b, parity, WAIT_LIMIT);
 }
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
                                             uint64_t* bar) {

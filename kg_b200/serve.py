@@ -15,6 +15,13 @@ path (kg_rk4 on its own handle), the baseline the batched form is compared
 with.  `precision="mixed"` runs the batched solves with the FP32 stencil RHS and
 the FP64 state update (kg_batch_set_precision).
 
+Failures stay with the request that caused them: a request whose solve cannot
+be created (bad parameters, device memory exhausted) is refused and reported,
+one withdrawn by its `cancel_at` time leaves at the next quantum boundary with
+the waveform it has so far, and a solve whose waveform sample is not finite is
+retired as failed; in each case its device memory returns to the admission
+budget and the other solves run on.
+
 The reference has no serving layer (one MPI job per solve); the solve itself
 is the reference's RK4 path (MoL/lines_method_lib.f90:411-474) and the
 waveform is its detector projection (MoL/diagnostic_lib.f90:231-250).
@@ -41,6 +48,7 @@ class Request:
     steps: int
     r0: float = 10.0
     sigma: float = 1.5
+    cancel_at: float | None = None  # withdrawn at this time (seconds after the start), if set
 
     def grid(self):
         return dict(Nx=self.Nr, Ny=self.Ntheta + 1, Nz=2 * self.Ntheta + 1, xmin=1.8, xmax=1.8 + 0.1 * self.Nr)
@@ -59,6 +67,8 @@ class Result:
     steps: int
     times: np.ndarray = field(repr=False)
     alm: np.ndarray = field(repr=False)   # (samples, 2L+1, L+1) complex
+    status: str = "done"                  # "done", "cancelled" or "failed"
+    reason: str = ""
 
     @property
     def latency(self):
@@ -101,6 +111,15 @@ def _make_solve(req, l_max, device):
     return s
 
 
+# what creating a solve raises when its parameters are refused (KG_EINVAL) or its
+# device memory cannot be had
+_CREATE_ERRORS = (RuntimeError, ValueError, MemoryError)
+
+
+def _ended(r, admitted, done, ts, alms, status, reason):
+    return Result(r.rid, r.arrival, admitted, done, r.steps, np.array(ts), np.array(alms), status, reason)
+
+
 def _bytes_estimate(req, precision="fp64"):
     """device bytes of a live solve: u (5 FP64 variables, 80 B per point), the
     RK4 stage buffers and increment sum (15 variables: FP64 240 B, mixed FP32
@@ -138,17 +157,34 @@ class Server:
             if r.arrival > now:
                 time.sleep(r.arrival - now)
             admitted = time.perf_counter() - t0
-            s = _make_solve(r, self.l_max, self.device)
+            if _bytes_estimate(r, self.precision) > self.budget:
+                results.append(_ended(r, admitted, admitted, [], [], "failed", "exceeds the HBM budget alone"))
+                continue
+            if r.cancel_at is not None and r.cancel_at <= admitted:
+                results.append(_ended(r, admitted, admitted, [], [], "cancelled", "withdrawn before admission"))
+                continue
+            try:
+                s = _make_solve(r, self.l_max, self.device)
+            except _CREATE_ERRORS as e:
+                results.append(_ended(r, admitted, admitted, [], [], "failed", f"not created: {e}"))
+                continue
             s.precision = self.precision
             ts, alms = [], []
             done_steps = 0
+            status, reason = "done", ""
             while done_steps < r.steps:
+                if r.cancel_at is not None and time.perf_counter() - t0 >= r.cancel_at:
+                    status, reason = "cancelled", f"withdrawn after {done_steps} steps"
+                    break
                 s.rk4(nsteps=self.q)
                 done_steps += self.q
                 alms.append(self._sample(s))
                 ts.append(s.t)
+                if not np.all(np.isfinite(alms[-1])):
+                    status, reason = "failed", f"non-finite waveform after {done_steps} steps"
+                    break
             done = time.perf_counter() - t0
-            results.append(Result(r.rid, r.arrival, admitted, done, r.steps, np.array(ts), np.array(alms)))
+            results.append(_ended(r, admitted, done, ts, alms, status, reason))
             s.close()
         return self._summary(results, time.perf_counter() - t0)
 
@@ -177,10 +213,24 @@ class Server:
             # solves are created and join the batch while the quantum runs; they
             # are appended after the live members, and step from the next quantum
             joined = []
-            while pending and len(live) + len(joined) < self.max_live and \
-                    used + _bytes_estimate(pending[0], self.precision) <= self.budget:
+            while pending and len(live) + len(joined) < self.max_live:
+                need = _bytes_estimate(pending[0], self.precision)
+                now = time.perf_counter() - t0
+                if need > self.budget:
+                    r = pending.popleft()
+                    results.append(_ended(r, now, now, [], [], "failed", "exceeds the HBM budget alone"))
+                    continue
+                if used + need > self.budget:
+                    break
                 r = pending.popleft()
-                s = _make_solve(r, self.l_max, self.device)
+                if r.cancel_at is not None and r.cancel_at <= now:
+                    results.append(_ended(r, now, now, [], [], "cancelled", "withdrawn before admission"))
+                    continue
+                try:
+                    s = _make_solve(r, self.l_max, self.device)
+                except _CREATE_ERRORS as e:
+                    results.append(_ended(r, now, now, [], [], "failed", f"not created: {e}"))
+                    continue
                 batch.add(s)
                 used += _bytes_estimate(r, self.precision)
                 joined.append([r, s, 0, time.perf_counter() - t0, [], []])
@@ -194,24 +244,27 @@ class Server:
                     entry[2] += self.q
                     entry[5].append(a[0].copy())
                     entry[4].append(s.t)
-                    if entry[2] >= r.steps:
-                        done = time.perf_counter() - t0
-                        batch.remove(s)
-                        results.append(Result(r.rid, r.arrival, entry[3], done, r.steps, np.array(entry[4]),
-                                              np.array(entry[5])))
-                        used -= _bytes_estimate(r, self.precision)
-                        s.close()
-                    else:
+                    now = time.perf_counter() - t0
+                    status = None
+                    if not np.all(np.isfinite(entry[5][-1])):
+                        status, reason = "failed", f"non-finite waveform after {entry[2]} steps"
+                    elif entry[2] >= r.steps:
+                        status, reason = "done", ""
+                    elif r.cancel_at is not None and now >= r.cancel_at:
+                        status, reason = "cancelled", f"withdrawn after {entry[2]} steps"
+                    if status is None:
                         still.append(entry)
+                        continue
+                    batch.remove(s)
+                    results.append(_ended(r, entry[3], now, entry[4], entry[5], status, reason))
+                    used -= _bytes_estimate(r, self.precision)
+                    s.close()
             live = still + joined
-            if not live:
-                if pending:
-                    # admission ran before this quantum's retirements freed their memory;
-                    # the next pass admits unless the head request alone exceeds the budget
-                    if _bytes_estimate(pending[0], self.precision) > self.budget:
-                        raise RuntimeError("a single request exceeds the HBM budget")
-                elif i_next < len(reqs):
-                    time.sleep(max(0.0, reqs[i_next].arrival - (time.perf_counter() - t0)))
+            # with nothing live and nothing pending, wait for the next arrival (with
+            # requests pending, admission ran before this quantum's retirements freed
+            # their memory, and the next pass admits them)
+            if not live and not pending and i_next < len(reqs):
+                time.sleep(max(0.0, reqs[i_next].arrival - (time.perf_counter() - t0)))
         wall = time.perf_counter() - t0
         batch.close()
         out = self._summary(results, wall)
@@ -220,11 +273,16 @@ class Server:
 
     @staticmethod
     def _summary(results, wall):
-        lat = np.array([r.latency for r in results])
-        return {"results": sorted(results, key=lambda r: r.rid), "wall_s": wall, "completed": len(results),
-                "solves_per_s": len(results) / wall if wall > 0 else 0.0,
+        """rates and latencies over the requests served to the end; the
+        cancelled and failed ones are listed with their reasons"""
+        ok = [r for r in results if r.status == "done"]
+        lat = np.array([r.latency for r in ok])
+        return {"results": sorted(ok, key=lambda r: r.rid), "wall_s": wall, "completed": len(ok),
+                "solves_per_s": len(ok) / wall if wall > 0 else 0.0,
                 "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
-                "p99_s": float(np.percentile(lat, 99)) if len(lat) else None}
+                "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+                "cancelled": sorted((r for r in results if r.status == "cancelled"), key=lambda r: r.rid),
+                "failed": sorted((r for r in results if r.status == "failed"), key=lambda r: r.rid)}
 
 
 def waveform_error(a, b, floor=1e-10):

@@ -13,9 +13,19 @@ class FakeSolve:
         self.steps = 0
         self.t = 0.0
         self.closed = False
+        self.precision = "fp64"
 
     def close(self):
         self.closed = True
+
+    # the single-solve path (plain mode)
+    def rk4(self, nsteps):
+        self.steps += nsteps
+        self.t += nsteps * 0.1
+        assert self.steps <= self.req.steps
+
+    def proyector_detectors(self):
+        return FakeBatch.sample(self)
 
 
 class FakeBatch:
@@ -46,14 +56,19 @@ class FakeBatch:
             m.t += n * 0.1
             assert m.steps <= m.req.steps, "a solve stepped past its request"
 
+    nan_at = {}  # rid -> step count from which the solve's samples are NaN (a state gone bad)
+
+    @staticmethod
+    def sample(m):
+        # one (n_det, 2L+1, L+1) block; [0, 0, 0] encodes the solve and its step count
+        a = np.zeros((2, 3, 2), np.complex128)
+        a[0, 0, 0] = m.req.rid + 1j * m.steps
+        if m.req.rid in FakeBatch.nan_at and m.steps >= FakeBatch.nan_at[m.req.rid]:
+            a[0, 1, 1] = np.nan
+        return a
+
     def proyector_detectors(self):
-        # one (n_det, 2L+1, L+1) block per member; [0, 0, 0] encodes the solve and its step count
-        out = []
-        for m in self.members:
-            a = np.zeros((2, 3, 2), np.complex128)
-            a[0, 0, 0] = m.req.rid + 1j * m.steps
-            out.append(a)
-        return out
+        return [FakeBatch.sample(m) for m in self.members]
 
     def close(self):
         self.closed = True
@@ -71,6 +86,7 @@ def served(monkeypatch):
         return s
 
     FakeBatch.instances.clear()
+    FakeBatch.nan_at = {}
     monkeypatch.setattr(serve, "_make_solve", make)
     monkeypatch.setattr(kg_b200.batch, "Batch", FakeBatch)
     return serve, made
@@ -116,12 +132,73 @@ def test_batched_loop_budget_never_exceeded(served, monkeypatch):
     assert max(live_bytes) <= budget
 
 
-def test_request_larger_than_budget_is_refused(served):
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_request_larger_than_budget_is_refused(served, mode):
+    """a request that alone exceeds the HBM budget is refused and reported; the
+    others are served"""
     serve, made = served
-    reqs = serve.draw_requests(seed=5, rate=1e6, count=2, nr=(64, 64), nr_step=16, ntheta=(16,),
+    reqs = serve.draw_requests(seed=5, rate=1e6, count=3, nr=(64, 64), nr_step=16, ntheta=(16,),
                                steps=(10, 10), quantum=10)
-    with pytest.raises(RuntimeError):
-        serve.Server(mode="batched", hbm_budget=serve._bytes_estimate(reqs[0]) / 2).run(reqs)
+    big = serve.Request(rid=99, arrival=0.0, Nr=4096, Ntheta=64, m=0.1, seed=1, steps=10)
+    budget = 2 * serve._bytes_estimate(reqs[0])
+    assert serve._bytes_estimate(big) > budget
+    out = serve.Server(mode=mode, hbm_budget=budget).run(reqs + [big])
+    assert out["completed"] == 3
+    assert [(r.rid, r.reason) for r in out["failed"]] == [(99, "exceeds the HBM budget alone")]
+    assert all(s.req.rid != 99 for s in made)
+
+
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_faults_stay_with_their_request(served, monkeypatch, mode):
+    """Host-injected faults, none on the GPU: a malformed request (creation refuses
+    its parameters), an allocation failure, a request withdrawn before admission,
+    one withdrawn while it runs, and a solve whose state goes non-finite.  Each is
+    reported with its reason, its solve (if any) is closed and leaves the batch,
+    its memory returns to the budget, and every other request is served in full."""
+    import time
+    serve, made = served
+    reqs = serve.draw_requests(seed=6, rate=1e6, count=12, nr=(16, 48), nr_step=16, ntheta=(8,),
+                               steps=(60, 60), quantum=10)
+    reqs[1].cancel_at = 0.0                  # withdrawn before admission
+    reqs[0].cancel_at = 0.005                # withdrawn after its first quantum (each quantum takes 20 ms)
+    FakeBatch.nan_at = {6: 30}               # its state goes bad during its third quantum
+    fake_make = serve._make_solve
+
+    def make(req, l_max, device):
+        if req.rid == 2:
+            raise ValueError("Nx must be at least 4")                   # malformed
+        if req.rid == 3:
+            raise MemoryError("device allocation of 1e13 bytes failed")  # out of device memory
+        return fake_make(req, l_max, device)
+
+    monkeypatch.setattr(serve, "_make_solve", make)
+    orig_rk4, orig_srk4 = FakeBatch.rk4, FakeSolve.rk4
+
+    def slow(f):
+        def g(self, *a, **k):
+            time.sleep(0.02)
+            return f(self, *a, **k)
+        return g
+
+    monkeypatch.setattr(FakeBatch, "rk4", slow(orig_rk4))
+    monkeypatch.setattr(FakeSolve, "rk4", slow(orig_srk4))
+    budget = 3.5 * max(serve._bytes_estimate(r) for r in reqs)
+    out = serve.Server(mode=mode, hbm_budget=budget, save_every=10).run(reqs)
+    failed = {r.rid: r.reason for r in out["failed"]}
+    cancelled = {r.rid: r for r in out["cancelled"]}
+    assert failed[2].startswith("not created: Nx must be at least 4")
+    assert failed[3].startswith("not created: device allocation")
+    assert failed[6] == "non-finite waveform after 30 steps"
+    assert set(failed) == {2, 3, 6}
+    assert cancelled[1].reason == "withdrawn before admission" and len(cancelled[1].alm) == 0
+    assert cancelled[0].reason.startswith("withdrawn after") and 0 < len(cancelled[0].alm) < 6
+    assert set(cancelled) == {0, 1}
+    assert out["completed"] == len(reqs) - 5
+    for res in out["results"]:
+        assert res.status == "done" and len(res.alm) == 6
+    assert all(s.closed for s in made)
+    if mode == "batched":
+        assert not FakeBatch.instances[-1].members
 
 
 def test_tuner_candidates_cover_both_dispatches():
