@@ -10,10 +10,11 @@ diagnostics.
 `autotune` picks how a batch runs by timing candidates on scratch solves of
 the same grid shapes (the live solves are never advanced by the tuning):
   * dispatch 0, one persistent launch per stage over all members: the phi
-    planes per work item (kchunk) and the number of persistent CTAs;
+    planes per work item (kchunk), the number of persistent CTAs and the tile
+    height (32 x 8 or 32 x 4 (r, theta) tiles);
   * dispatch 1, every member's own single-solve kernels on its own stream, all
     members concurrently: the stage-kernel form, i.e. the tile shape of the
-    stage kernels (32 x 8 (r, theta) tiles fed by TMA, 32 x 8 tiles with
+    stage kernels (32 x 8 or 32 x 4 tiles fed by TMA, 32 x 8 tiles with
     register prefetch, or one thread per point in rows of 128).
 """
 from __future__ import annotations

@@ -15,8 +15,8 @@
 // and write the stage (40) and the sum (40); stage 4 reads the stage (40), u
 // (80) and the sum (40) and writes u (80): 880 B against 1360 B in FP64.
 //
-// Kernel organisation is that of the FP64 TMA form: a CTA owns a 32 x 8 tile
-// of (r, theta) columns and marches through a chunk of phi planes; each plane
+// Kernel organisation is that of the FP64 TMA form: a CTA owns a 32 x 8 (or
+// 32 x 4) tile of (r, theta) columns and marches through a chunk of phi planes; each plane
 // of the five stencil inputs with its r (+-2) and theta (+-1) halo arrives by
 // one cp.async.bulk.tensor box into a 3-deep shared-memory ring tracked by
 // mbarriers with bounded waits; the point-wise operands are prefetched into L2

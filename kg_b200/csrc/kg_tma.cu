@@ -2,8 +2,11 @@
 //
 // Same arithmetic as kg_stencil.cu and kg_march.cu, bit for bit; the memory
 // side is organised for Blackwell:
-//   * a CTA owns a 32 x 8 tile of (r, theta) columns and marches through a
-//     chunk of phi planes;
+//   * a CTA owns a 32 x 8 tile of (r, theta) columns (32 x 4 for the RK4
+//     stages when asked: twice the tiles of a small grid) and marches through
+//     a chunk of phi planes; a warp whose lanes all lie two points inside the
+//     array in r with beta^r > 0 takes the centred and forward-upwind
+//     differences without per-lane branches;
 //   * every plane the CTA needs -- the tile with a +-2 r halo and a +-1 theta
 //     halo, all five stencil inputs -- is brought into a 3-deep shared-memory
 //     ring by the tensor-memory accelerator (cp.async.bulk.tensor, two boxes
