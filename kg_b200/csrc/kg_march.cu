@@ -42,6 +42,9 @@ __device__ __forceinline__ double ddiv(double a, double b, double rb) {
 __device__ __forceinline__ double2 cdivm(double2 a, double b, double rb) {
   return c2(ddiv(a.x, b, rb), ddiv(a.y, b, rb));
 }
+// the stage combinations' divisions by 3 (SSP-RK3) and 6 (RK4) take the same
+// route, from the correctly rounded reciprocals
+constexpr double kThird = 1.0 / 3.0, kSixth = 1.0 / 6.0;
 
 struct MarchArgs {
   Grid g;
@@ -316,7 +319,7 @@ __global__ void __launch_bounds__(TI * TJ, 2) march_kernel(MarchArgs a) {
           } else if (KIND == ST_RK3_2) {
             res = cadd(rmul(0.750, b), rmul(0.250, cadd(fcu[v], rmul(dt, r[v]))));
           } else if (KIND == ST_RK3_3) {
-            res = cadd(cdivr(b, 3.0), cdivr(rmul(2.0, cadd(fcu[v], rmul(dt, r[v]))), 3.0));
+            res = cadd(cdivm(b, 3.0, kThird), cdivm(rmul(2.0, cadd(fcu[v], rmul(dt, r[v]))), 3.0, kThird));
           } else if (KIND == ST_RK4_1) {
             const double2 kk = rmul(dt, r[v]);
             a.acc[o] = kk;
@@ -331,7 +334,7 @@ __global__ void __launch_bounds__(TI * TJ, 2) march_kernel(MarchArgs a) {
             res = cadd(b, kk);
           } else {  // ST_RK4_4
             const double2 kk = rmul(dt, r[v]);
-            res = cadd(b, cdivr(cadd(a.acc[o], kk), 6.0));
+            res = cadd(b, cdivm(cadd(a.acc[o], kk), 6.0, kSixth));
           }
           a.out[o] = res;
         }
