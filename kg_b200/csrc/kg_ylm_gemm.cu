@@ -223,37 +223,85 @@ __global__ void __launch_bounds__(128, 1)
 // operand preparation
 
 // phi on every vertex shell (domain_to_sph at all r), split into BF16 head/tail:
-// A rows 0..Nx-1 = Re, Nx..2Nx-1 = Im, columns (jv, kv) -> jv + Ny kv, row pitch Kp
-__global__ void shells_to_a_kernel(Grid g, const double2* __restrict__ u, ShellInterp si, int Nx, int Ny, int Nz,
-                                   int Kp, __nv_bfloat16* Ahi, __nv_bfloat16* Alo, double2* Fout) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long n = (long long)Nx * Ny * Nz;
-  if (t >= n) return;
-  const int jv = (int)(t % Ny);
-  const long long r2 = t / Ny;
-  const int kv = (int)(r2 % Nz);
-  const int iv = (int)(r2 / Nz);  // 0-based shell: vertex r index iv+1 -> evolution ii = iv
-  const int ir = iv, ith = si.i_th[jv], iph = si.i_ph[kv];
-  double2 f;
-  const int fl = si.th_flag[jv];
-  if (fl == 1) f = u[off3(g, ir, 0, iph)];
-  else if (fl == 2) f = u[off3(g, ir, g.NJ - 1, iph)];
-  else {
-    const double wt = si.w_th[jv], wp = si.w_ph[kv];
-    const int ip1 = iph + 1;
-    const double2 f00 = cadd(rmul(1.0 - wp, u[off3(g, ir, ith, iph)]), rmul(wp, u[off3(g, ir, ith, ip1)]));
-    const double2 f01 = cadd(rmul(1.0 - wp, u[off3(g, ir, ith + 1, iph)]), rmul(wp, u[off3(g, ir, ith + 1, ip1)]));
-    f = cadd(rmul(1.0 - wt, f00), rmul(wt, f01));
+// A rows 0..Nx-1 = Re, Nx..2Nx-1 = Im, columns (jv, kv) -> jv + Ny kv, row pitch Kp.
+// A block transposes a tile of 32 shells x 64 sphere columns through shared
+// memory: each warp reads the interpolation points of one sphere column on 32
+// consecutive shells (consecutive r, so the loads are coalesced), and each warp
+// then writes 64 consecutive columns of one shell's A rows.  The value of each
+// point is the same expression as the one-point-per-thread form gave.
+constexpr int SA_R = 32, SA_C = 64;
+__global__ void __launch_bounds__(256) shells_to_a_kernel(Grid g, const double2* __restrict__ u, ShellInterp si,
+                                                          int Nx, int Ny, int Nz, int Kp, __nv_bfloat16* Ahi,
+                                                          __nv_bfloat16* Alo, double2* Fout) {
+  __shared__ double2 T[SA_C][SA_R + 1];  // odd pitch in 16-byte units: conflict-free column reads
+  __shared__ int s_ith[SA_C], s_iph[SA_C], s_fl[SA_C];
+  __shared__ double s_wt[SA_C], s_wp[SA_C];
+  const int K = Ny * Nz;
+  const int iv0 = blockIdx.x * SA_R, col0 = blockIdx.y * SA_C;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // the interpolation data of the block's sphere columns, once
+  if (threadIdx.x < SA_C) {
+    const int col = col0 + threadIdx.x;
+    if (col < K) {
+      const int jv = col % Ny, kv = col / Ny;
+      s_ith[threadIdx.x] = si.i_th[jv];
+      s_iph[threadIdx.x] = si.i_ph[kv];
+      s_fl[threadIdx.x] = si.th_flag[jv];
+      s_wt[threadIdx.x] = si.w_th[jv];
+      s_wp[threadIdx.x] = si.w_ph[kv];
+    }
   }
-  const long long col = jv + (long long)Ny * kv;
-  if (Fout) Fout[(long long)iv * Ny * Nz + col] = f;
-  if (Ahi) {
-    const float re = (float)f.x, im = (float)f.y;
-    const __nv_bfloat16 rh = __float2bfloat16_rn(re), ih = __float2bfloat16_rn(im);
-    Ahi[(long long)iv * Kp + col] = rh;
-    Alo[(long long)iv * Kp + col] = __float2bfloat16_rn(re - __bfloat162float(rh));
-    Ahi[(long long)(Nx + iv) * Kp + col] = ih;
-    Alo[(long long)(Nx + iv) * Kp + col] = __float2bfloat16_rn(im - __bfloat162float(ih));
+  __syncthreads();
+#pragma unroll 4
+  for (int cc = warp; cc < SA_C; cc += 8) {
+    const int col = col0 + cc, iv = iv0 + lane;  // 0-based shell: vertex r index iv+1 -> evolution ii = iv
+    double2 f = c2(0.0, 0.0);
+    if (col < K && iv < Nx) {
+      const int ir = iv, ith = s_ith[cc], iph = s_iph[cc];
+      const int fl = s_fl[cc];
+      if (fl == 1) f = u[off3(g, ir, 0, iph)];
+      else if (fl == 2) f = u[off3(g, ir, g.NJ - 1, iph)];
+      else {
+        const double wt = s_wt[cc], wp = s_wp[cc];
+        const int ip1 = iph + 1;
+        const double2 f00 = cadd(rmul(1.0 - wp, u[off3(g, ir, ith, iph)]), rmul(wp, u[off3(g, ir, ith, ip1)]));
+        const double2 f01 =
+            cadd(rmul(1.0 - wp, u[off3(g, ir, ith + 1, iph)]), rmul(wp, u[off3(g, ir, ith + 1, ip1)]));
+        f = cadd(rmul(1.0 - wt, f00), rmul(wt, f01));
+      }
+    }
+    T[cc][lane] = f;
+  }
+  __syncthreads();
+  for (int rr = warp; rr < SA_R; rr += 8) {
+    const int iv = iv0 + rr;
+    if (iv >= Nx) break;
+    if (Fout) {
+      for (int c = lane; c < SA_C; c += 32) {
+        const int col = col0 + c;
+        if (col < K) Fout[(long long)iv * K + col] = T[c][rr];
+      }
+    }
+    if (Ahi) {
+      // two adjacent columns per lane, stored as BF16 pairs (col0 and Kp are even)
+      const int c = 2 * lane, col = col0 + c;
+      if (col < K) {
+        const double2 f0 = T[c][rr];
+        const double2 f1 = (col + 1 < K) ? T[c + 1][rr] : c2(0.0, 0.0);  // K <= column < Kp: the zero pad
+        const float re0 = (float)f0.x, im0 = (float)f0.y, re1 = (float)f1.x, im1 = (float)f1.y;
+        const __nv_bfloat16 rh0 = __float2bfloat16_rn(re0), ih0 = __float2bfloat16_rn(im0);
+        const __nv_bfloat16 rh1 = __float2bfloat16_rn(re1), ih1 = __float2bfloat16_rn(im1);
+        const __nv_bfloat162 rh = __halves2bfloat162(rh0, rh1), ih = __halves2bfloat162(ih0, ih1);
+        const __nv_bfloat162 rl = __halves2bfloat162(__float2bfloat16_rn(re0 - __bfloat162float(rh0)),
+                                                     __float2bfloat16_rn(re1 - __bfloat162float(rh1)));
+        const __nv_bfloat162 il = __halves2bfloat162(__float2bfloat16_rn(im0 - __bfloat162float(ih0)),
+                                                     __float2bfloat16_rn(im1 - __bfloat162float(ih1)));
+        *reinterpret_cast<__nv_bfloat162*>(Ahi + (long long)iv * Kp + col) = rh;
+        *reinterpret_cast<__nv_bfloat162*>(Alo + (long long)iv * Kp + col) = rl;
+        *reinterpret_cast<__nv_bfloat162*>(Ahi + (long long)(Nx + iv) * Kp + col) = ih;
+        *reinterpret_cast<__nv_bfloat162*>(Alo + (long long)(Nx + iv) * Kp + col) = il;
+      }
+    }
   }
 }
 
@@ -284,38 +332,58 @@ __global__ void ylm_b_kernel(int L, int Ny, int Nz, int Kp, const double* __rest
   Blo[o] = __float2bfloat16_rn(v - __bfloat162float(h));
 }
 
-// a_lm(l, m, shell) from the GEMM blocks P Q / R T
+// a_lm(l, m, shell) from the GEMM blocks P Q / R T.  One thread per (mode with
+// m >= 0, shell), modes fastest, so the reads of each split's partial rows are
+// coalesced; the thread writes a_l,m and a_l,-m.  The entries with |m| > l are
+// zeroed before the launch.
 __global__ void ylm_assemble_kernel(const float* __restrict__ C, int ldc, long long csplit, int nsplit, int Nx,
                                     int L, double dydz, double2* __restrict__ alm) {
+  const int Nm = (L + 1) * (L + 2) / 2;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int NL = L + 1, NM = 2 * L + 1;
-  const long long n = (long long)NL * NM * Nx;
-  if (t >= n) return;
-  const int l = (int)(t % NL);
-  const int mi = (int)((t / NL) % NM);
-  const int iv = (int)(t / ((long long)NL * NM));
-  const int m = mi - L;
-  double2 out = c2(0.0, 0.0);
-  if (m >= -l && m <= l) {
-    const int am = m < 0 ? -m : m;
-    const int Nm = (L + 1) * (L + 2) / 2;
-    const int mode = l * (l + 1) / 2 + am;
-    double P = 0.0, Q = 0.0, R = 0.0, T = 0.0;  // the split partials added in FP64, in split order
-    for (int z = 0; z < nsplit; ++z) {
-      const float* Cz = C + (long long)z * csplit;
-      P += (double)Cz[(size_t)iv * ldc + mode];
-      Q += (double)Cz[(size_t)iv * ldc + Nm + mode];
-      R += (double)Cz[(size_t)(Nx + iv) * ldc + mode];
-      T += (double)Cz[(size_t)(Nx + iv) * ldc + Nm + mode];
+  if (t >= (long long)Nm * Nx) return;
+  const int mode = (int)(t % Nm);
+  const int iv = (int)(t / Nm);
+  int l = (int)((sqrt(8.0 * mode + 1.0) - 1.0) * 0.5);  // mode = l (l + 1) / 2 + m
+  while (l * (l + 1) / 2 > mode) --l;
+  while ((l + 1) * (l + 2) / 2 <= mode) ++l;
+  const int am = mode - l * (l + 1) / 2;
+  // the split partials added in FP64, in split order; four splits' loads are
+  // issued before their sums, so a thread has sixteen loads in flight
+  double P = 0.0, Q = 0.0, R = 0.0, T = 0.0;
+  const float* c0 = C + (size_t)iv * ldc + mode;
+  const float* c1 = C + (size_t)(Nx + iv) * ldc + mode;
+  int z = 0;
+  for (; z + 4 <= nsplit; z += 4) {
+    float p[4], q[4], r[4], t4[4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const long long o = (long long)(z + w) * csplit;
+      p[w] = __ldg(c0 + o);
+      q[w] = __ldg(c0 + o + Nm);
+      r[w] = __ldg(c1 + o);
+      t4[w] = __ldg(c1 + o + Nm);
     }
-    if (m >= 0) out = c2(P + T, R - Q);
-    else {
-      const double sg = (am & 1) ? -1.0 : 1.0;
-      out = c2(sg * (P - T), sg * (R + Q));
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      P += (double)p[w];
+      Q += (double)q[w];
+      R += (double)r[w];
+      T += (double)t4[w];
     }
-    out = rmul(dydz, out);
   }
-  alm[t] = out;
+  for (; z < nsplit; ++z) {
+    const long long o = (long long)z * csplit;
+    P += (double)__ldg(c0 + o);
+    Q += (double)__ldg(c0 + o + Nm);
+    R += (double)__ldg(c1 + o);
+    T += (double)__ldg(c1 + o + Nm);
+  }
+  const int NL = L + 1, NM = 2 * L + 1;
+  alm[((long long)iv * NM + (L + am)) * NL + l] = rmul(dydz, c2(P + T, R - Q));
+  if (am > 0) {
+    const double sg = (am & 1) ? -1.0 : 1.0;
+    alm[((long long)iv * NM + (L - am)) * NL + l] = rmul(dydz, c2(sg * (P - T), sg * (R + Q)));
+  }
 }
 
 // FP64 projection over all shells.  One block per (l-chunk, m >= 0, shell): the
@@ -448,8 +516,8 @@ int launch_ylm_gemm(const __nv_bfloat16* Ahi, const __nv_bfloat16* Alo, const __
 
 void launch_shells_to_a(const Grid& g, const double2* u, const ShellInterp& si, int Nx, int Ny, int Nz, int Kp,
                         __nv_bfloat16* Ahi, __nv_bfloat16* Alo, double2* F, cudaStream_t st) {
-  const long long n = (long long)Nx * Ny * Nz;
-  shells_to_a_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, u, si, Nx, Ny, Nz, Kp, Ahi, Alo, F);
+  const dim3 grid((Nx + SA_R - 1) / SA_R, (Ny * Nz + SA_C - 1) / SA_C);
+  shells_to_a_kernel<<<grid, 256, 0, st>>>(g, u, si, Nx, Ny, Nz, Kp, Ahi, Alo, F);
 }
 
 void launch_ylm_b(int L, int Ny, int Nz, int Kp, const double* normP, const double* cosm, const double* sinm,
@@ -461,7 +529,8 @@ void launch_ylm_b(int L, int Ny, int Nz, int Kp, const double* normP, const doub
 
 void launch_ylm_assemble(const float* C, int ldc, long long csplit, int nsplit, int Nx, int L, double dydz,
                          double2* alm, cudaStream_t st) {
-  const long long n = (long long)(L + 1) * (2 * L + 1) * Nx;
+  cudaMemsetAsync(alm, 0, (size_t)(L + 1) * (2 * L + 1) * Nx * sizeof(double2), st);  // |m| > l
+  const long long n = (long long)(L + 1) * (L + 2) / 2 * Nx;
   ylm_assemble_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(C, ldc, csplit, nsplit, Nx, L, dydz, alm);
 }
 
