@@ -7,6 +7,7 @@
     python -m kg_b200.profile_cases batch      [--solves N] [--precision fp64|mixed] [--mix serving|c3] [--steps K]
     python -m kg_b200.profile_cases refine     [--grid Nx,Ny,Nz] [--steps K]
     python -m kg_b200.profile_cases diag       [--grid Nx,Ny,Nz] [--steps K]
+    python -m kg_b200.profile_cases steppers   [--grid Nx,Ny,Nz] [--steps K]
 
 Each case builds seeded synthetic input on the device, runs K steps and exits
 0 (or raises); the sizes default to a few GB of device memory, larger than
@@ -25,6 +26,11 @@ L2, so a profiler capture of one launch is representative and ends quickly.
   diag:       the diagnostics of the evolve loop K times: density, the mass
               integral (warp-shuffle partial sums), the currents and the
               detector projection
+  steppers:   PIRK2, PIRK3, SSP-RK3 and RK4 on the benchmark grid (default
+              2048 x 129 x 257), K steps each after warm-up, with every kernel
+              kind timed by CUDA events; prints one line per stepper with the
+              time per launch and the fraction of the measured HBM copy rate
+              (MEASURED_PEAKS.json, else 6650 GB/s) its algorithmic bytes reach
 """
 from __future__ import annotations
 
@@ -44,9 +50,52 @@ def _device_ic(s, Nx, Ny, Nz, xmin, xmax, seed=7):
     s.synchronize()
 
 
-def main(argv=None):
+# algorithmic bytes per stored point of each stage kernel (FP64 complex: 16 B per variable)
+STAGE_BYTES = {"stage_pirk_s1_fused": 176, "stage_pirk_s1_psi": 144, "stage_pirk_s1_pi": 112, "stage_pirk2_s2": 240,
+               "stage_pirk3_s2_psi": 208, "stage_pirk3_s2_pi": 128, "stage_pirk3_s3": 240,
+               "stage_rk3_1": 160, "stage_rk3_2": 240, "stage_rk3_3": 240,
+               "stage_rk4_1": 240, "stage_rk4_2": 400, "stage_rk4_3": 400, "stage_rk4_4": 320}
+
+
+def _steppers(a):
+    import json
+    import os
+    from .lines_method import ScalarField
+    Nx, Ny, Nz = _grid(a.grid, (2048, 129, 257))
+    xmax = 1.8 + 0.1944 * Nx
+    s = ScalarField(Nx, Ny, Nz, 1.8, xmax, 0.25, m=0.3, device=0, n_det=2, l_max=0)
+    _device_ic(s, Nx, Ny, Nz, 1.8, xmax)
+    lib = s._lib
+    nk = lib.kg_profile_kinds()
+    names = [lib.kg_profile_kind_name(i).decode() for i in range(nk)]
+    pts = (Nx + 5) * (Ny + 5) * (Nz + 1)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    peaks = os.path.join(root, "MEASURED_PEAKS.json")
+    peak = float(json.load(open(peaks)).get("hbm_gbs", 6650.0)) if os.path.exists(peaks) else 6650.0
+    ms = (C.c_double * nk)()
+    cnt = (C.c_longlong * nk)()
+    steps = max(a.steps, 2)
+    for meth in ("pirk2", "pirk3", "rk3", "rk4"):
+        run = getattr(s, meth)
+        step = (lambda n: run(nsteps=n)) if meth.startswith("rk") else run
+        step(4)  # buffers and the captured graphs of both Pi-slot parities
+        s.synchronize()
+        lib.kg_profile_enable(s.handle, 1)
+        lib.kg_profile_read(s.handle, ms, cnt)
+        step(steps)
+        s.synchronize()
+        lib.kg_profile_read(s.handle, ms, cnt)
+        lib.kg_profile_enable(s.handle, 0)
+        out = {}
+        for i in range(nk):
+            if cnt[i]:
+                per = ms[i] / cnt[i]
+                b = STAGE_BYTES.get(names[i], 0) * pts
+                out[names[i]] = {"ms": round(per, 3), "hbm_frac": round(b / (per / 1e3) / 1e9 / peak, 3) if b else None}
+        print(meth, json.dumps(out))
+
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["pirk", "mixed", "proj", "configured", "batch", "refine", "diag"])
+    ap.add_argument("case", choices=["pirk", "mixed", "proj", "configured", "batch", "refine", "diag", "steppers"])
     ap.add_argument("--lmax", type=int, default=64)
     ap.add_argument("--variant", type=int, default=3)
     ap.add_argument("--grid", default=None)
@@ -110,6 +159,8 @@ def main(argv=None):
         for _ in range(a.steps):
             b.rk4(1)
         b.synchronize()
+    elif a.case == "steppers":
+        _steppers(a)
     elif a.case == "diag":
         Nx, Ny, Nz = _grid(a.grid, (512, 129, 257))
         xmax = 1.8 + 0.1944 * Nx
