@@ -94,6 +94,8 @@ def _steppers(a):
                 out[names[i]] = {"ms": round(per, 3), "hbm_frac": round(b / (per / 1e3) / 1e9 / peak, 3) if b else None}
         print(meth, json.dumps(out))
 
+
+def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["pirk", "mixed", "proj", "configured", "batch", "refine", "diag", "steppers"])
     ap.add_argument("--lmax", type=int, default=64)
