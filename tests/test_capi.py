@@ -52,3 +52,13 @@ def test_invalid_params_rejected():
     assert lib.kg_destroy(None) == capi.KG_EINVAL
     assert lib.kg_profile_kinds() >= 13
     assert lib.kg_profile_kind_name(2) == b"stage_pirk2_s2"
+
+
+def test_integration_guide_names_every_entry_point():
+    """every function the header declares appears in the integration guide"""
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "kg_capi.h")).read()
+    guide = open(os.path.join(root, "INTEGRATION.md")).read()
+    names = set(re.findall(r"\b(kg_[a-z0-9_]+)\s*\(", header))
+    assert names and not sorted(n for n in names if n not in guide)
