@@ -825,14 +825,17 @@ def main():
 
     # ---- end to end through the C ABI with pinned host buffers
     state_bytes = 5 * 16 * stored_points(w)
-    host_u0 = torch.empty(u0.numel() * 2, dtype=torch.float64, pin_memory=True)
-    host_u0.copy_(torch.view_as_real(u0).reshape(-1))
-    host_out = torch.empty(host_u0.numel(), dtype=torch.float64, pin_memory=True)
+    # one pinned host buffer holds the input and then receives the result: kg_set_state
+    # returns after its copy has landed, so the download may overwrite it (5.7 GB of
+    # pinned memory per rank instead of 11.4)
+    host_u = None
+    if not args.no_e2e:
+        host_u = torch.empty(u0.numel() * 2, dtype=torch.float64, pin_memory=True)
+        host_u.copy_(torch.view_as_real(u0).reshape(-1))
     del u0
     mass = C.c_double(0.0)
     Dp = C.POINTER(C.c_double)
-    p_in = C.cast(C.c_void_p(host_u0.data_ptr()), Dp)
-    p_out = C.cast(C.c_void_p(host_out.data_ptr()), Dp)
+    p_in = p_out = C.cast(C.c_void_p(host_u.data_ptr()), Dp) if host_u is not None else None
     mol.density()
     barrier()
     torch.cuda.synchronize()
@@ -847,7 +850,7 @@ def main():
     f1.record(stream)
     f1.synchronize()
     e2e_ms = replicas.max_over_ranks(f0.elapsed_time(f1), world, device=f"cuda:{local}")
-    del host_u0, host_out, p_in, p_out  # 11 GB of pinned host memory, not needed by the legs below
+    del host_u, p_in, p_out  # pinned host memory, not needed by the legs below
 
     pts = interior_points(w)
     value = replicas.job_rate(pts * 2 * args.steps, world, el_ms)
