@@ -101,13 +101,17 @@ def _make_solve(req, l_max, device):
     g = req.grid()
     s = ScalarField(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], 0.25, m=req.m, l_max=l_max, n_det=2,
                     device=device)
-    u0, _ = shell_ylm_device(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], seed=req.seed,
-                             device=f"cuda:{max(device, 0)}", sigma=req.sigma, r0_range=(req.r0, req.r0))
-    s._ck(s._lib.kg_set_state_device(s.handle, 0, C.c_void_p(u0.data_ptr())))
-    s.synchronize()
-    del u0
-    r_max = s.r_max
-    s.set_detectors([0.8 * r_max, 0.8 * r_max])
+    try:
+        u0, _ = shell_ylm_device(g["Nx"], g["Ny"], g["Nz"], g["xmin"], g["xmax"], seed=req.seed,
+                                 device=f"cuda:{max(device, 0)}", sigma=req.sigma, r0_range=(req.r0, req.r0))
+        s._ck(s._lib.kg_set_state_device(s.handle, 0, C.c_void_p(u0.data_ptr())))
+        s.synchronize()
+        del u0
+        r_max = s.r_max
+        s.set_detectors([0.8 * r_max, 0.8 * r_max])
+    except BaseException:
+        s.close()  # the handle's device memory goes back at once, not at collection
+        raise
     return s
 
 
