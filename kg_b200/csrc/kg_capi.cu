@@ -1663,6 +1663,9 @@ int project_all(kg_solver* h, int L, int precision, double2** out_alm) {
     if (!h->ylm_b_ready) {
       KG_CK(cudaMemsetAsync(Bhi, 0, 2 * al(szB), h->stream));
       KG_CK(cudaMemsetAsync(Ahi, 0, 2 * al(szA), h->stream));
+      // the a_lm entries with |m| > l, which the assembly never writes (the FP64
+      // path writes them as zeros); the layout changes only with L or the buffer
+      KG_CK(cudaMemsetAsync(dalm, 0, al(szAlm), h->stream));
       {
         Prof pf(h, PK_YLM_PREP, 1);
         kg::launch_ylm_b(L, Ny, Nz, Kp, normP, cosm, sinm, h->sint, Bhi, Blo, h->stream);

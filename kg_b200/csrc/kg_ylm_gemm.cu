@@ -335,7 +335,7 @@ __global__ void ylm_b_kernel(int L, int Ny, int Nz, int Kp, const double* __rest
 // a_lm(l, m, shell) from the GEMM blocks P Q / R T.  One thread per (mode with
 // m >= 0, shell), modes fastest, so the reads of each split's partial rows are
 // coalesced; the thread writes a_l,m and a_l,-m.  The entries with |m| > l are
-// zeroed before the launch.
+// never written: the caller zeroes them once per buffer layout.
 __global__ void ylm_assemble_kernel(const float* __restrict__ C, int ldc, long long csplit, int nsplit, int Nx,
                                     int L, double dydz, double2* __restrict__ alm) {
   const int Nm = (L + 1) * (L + 2) / 2;
@@ -529,7 +529,6 @@ void launch_ylm_b(int L, int Ny, int Nz, int Kp, const double* normP, const doub
 
 void launch_ylm_assemble(const float* C, int ldc, long long csplit, int nsplit, int Nx, int L, double dydz,
                          double2* alm, cudaStream_t st) {
-  cudaMemsetAsync(alm, 0, (size_t)(L + 1) * (2 * L + 1) * Nx * sizeof(double2), st);  // |m| > l
   const long long n = (long long)(L + 1) * (L + 2) / 2 * Nx;
   ylm_assemble_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(C, ldc, csplit, nsplit, Nx, L, dydz, alm);
 }
