@@ -14,8 +14,9 @@ of the benchmarked solve.
 PIRK2 (MoL/lines_method_lib.f90:271-332) runs two steps, so the second step's
 stage 1 reads a non-zero previous-step Pi from the stage array; both the fused
 stage 1 (the default form) and the two-launch form are checked, state and stage
-arrays.  RK4 (:411-474) runs one step.  The mixed-precision RK4 step is held to
-1e-6 relative L2 of the FP64 step in phi and Pi on the same grid.
+arrays.  PIRK3 (:334-408) runs two steps (state and both stage arrays), SSP-RK3
+(:211-269) and RK4 (:411-474) one step each.  The mixed-precision RK4 step is
+held to 1e-6 relative L2 of the FP64 step in phi and Pi on the same grid.
 
 On this grid the shell's Gaussian tails reach the subnormal range at large r.
 There the tiled kernels' division by sqrt(gamma) (the correctly rounded
@@ -89,6 +90,33 @@ def test_full_grid_pirk2_matches_oracle(full_case):
         _assert_same_bits_above_underflow(s, ref_s, f"PIRK2 form {variant}, stage")
         del s
         dev.close()
+
+
+def test_full_grid_pirk3_and_rk3_match_oracle(full_case):
+    u0, ora = full_case
+    # PIRK stage 1 reads the previous step's Pi from the stage array: start it at
+    # zero, as in a fresh solver (the PIRK2 test ran on this oracle; u_stage_2 is
+    # written by PIRK3 alone)
+    ora.set_stage(np.zeros_like(u0))
+    ora.set_state(u0)
+    ora.pirk3(2)
+    ref_u, ref_s, ref_t = ora.get_state(), ora.get_stage(), ora.get_stage2()
+    dev = _solver()
+    dev.u = u0
+    dev.pirk3(2)
+    _assert_same_bits_above_underflow(dev.u, ref_u, "PIRK3, state")
+    _assert_same_bits_above_underflow(dev.u_stage, ref_s, "PIRK3, stage")
+    _assert_same_bits_above_underflow(dev.u_stage_2, ref_t, "PIRK3, second stage")
+    dev.close()
+    del ref_u, ref_s, ref_t
+    ora.set_state(u0)
+    ora.rk3(1)
+    ref = ora.get_state()
+    dev = _solver()
+    dev.u = u0
+    dev.rk3(nsteps=1)
+    _assert_same_bits_above_underflow(dev.u, ref, "SSP-RK3, state")
+    dev.close()
 
 
 def test_full_grid_rk4_matches_oracle_and_mixed(full_case):
