@@ -5,9 +5,9 @@
 // stage inputs u^n + c k are formed in FP64 and stored in FP32, the increments
 // k = dt rhs are kept as an FP32 sum k1 + 2 k2 + 2 k3, and the update
 // u^{n+1} = u^n + (k1 + 2 k2 + 2 k3 + k4) / 6 is computed in FP64.  Points of
-// the excision side (r index 0, 1) and of the two theta rows next to each pole
-// (where the 1/sqrt(gamma) ~ 1/sin(theta) factors are large) evaluate their
-// RHS in FP64 from the same stored values.
+// the excision side (r index 0, 1) and of the two interior theta rows next to
+// each pole (j = 1, 2 and Ny-2, Ny-1, where the 1/sqrt(gamma) ~ 1/sin(theta)
+// factors are largest) evaluate their RHS in FP64 from the same stored values.
 //
 // Bytes per stored point and step (5 complex variables, 8 B per FP32 value
 // pair, 16 B per FP64 pair): stage 1 reads u (80) and writes the stage (40)
@@ -365,8 +365,12 @@ __device__ __forceinline__ int mx_item(const CUtensorMap* tinp, const CUtensorMa
       own[6] = ldm(M.a_gpp, q);
     }
   }
-  // FP64 RHS at the excision side and next to the poles
-  const bool hp = (ii <= 1) || (jj <= 1) || (jj >= g.NJ - 2);
+  // FP64 RHS at the excision side (r index 0, 1) and on the two interior theta
+  // rows next to each pole (stored rows 3, 4 and NJ-5, NJ-4: j = 1, 2 and Ny-2,
+  // Ny-1, where 1/sqrt(gamma) ~ 1/sin(theta) is largest).  The three stored rows
+  // beyond each pole are ghost rows, which the pole fill overwrites from interior
+  // rows after every stage, so their RHS stays in FP32.
+  const bool hp = (ii <= 1) || (jj == 3) || (jj == 4) || (jj == g.NJ - 5) || (jj == g.NJ - 4);
   const bool fast =
       __all_sync(0xffffffffu, act && !hp && ii <= g.NI - 3 && (float)own[1] > 0.0f);  // warp-uniform
   auto EF = [&](const TIN* st, double2& E, double2& F) {
